@@ -1,0 +1,69 @@
+"""Build libfastfft_b200.so in-tree for sm_100a with nvcc (no torch dependency).
+
+Usage: python -m fastfft_b200.build [--jobs N] [--ptxas-verbose]
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+OBJ = PKG / "_build"
+LIB = PKG / "libfastfft_b200.so"
+SOURCES = ["twiddles.cu", "launch_rows.cu", "launch_cols.cu", "capi.cu"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+         "--expt-relaxed-constexpr"]
+
+
+def _compile(src: str, extra: list[str]) -> tuple[str, str]:
+    out = OBJ / (Path(src).stem + ".o")
+    cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", str(CSRC / src), "-o", str(out)]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{' '.join(cmd)}\n{p.stdout}\n{p.stderr}")
+    return str(out), p.stdout + p.stderr
+
+
+def _needs_build(extra: list[str]) -> bool:
+    if not LIB.exists():
+        return True
+    lib_t = LIB.stat().st_mtime
+    deps = list(CSRC.glob("*")) + [PKG.parent / "include" / "fastfft_capi.h", Path(__file__)]
+    return any(d.stat().st_mtime > lib_t for d in deps if d.exists())
+
+
+def build(jobs: int | None = None, ptxas_verbose: bool = False, force: bool = False) -> Path:
+    extra = ["-Xptxas", "-v"] if ptxas_verbose else []
+    if not force and not ptxas_verbose and not _needs_build(extra):
+        return LIB
+    OBJ.mkdir(exist_ok=True)
+    jobs = jobs or min(len(SOURCES), os.cpu_count() or 1)
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        results = list(ex.map(lambda s: _compile(s, extra), SOURCES))
+    if ptxas_verbose:
+        for _, log in results:
+            sys.stderr.write(log)
+    objs = [r[0] for r in results]
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", str(tmp), "-lcudart"]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{p.stdout}\n{p.stderr}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--jobs", type=int, default=None)
+    ap.add_argument("--ptxas-verbose", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    print(build(a.jobs, a.ptxas_verbose, a.force))

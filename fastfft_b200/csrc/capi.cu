@@ -1,0 +1,477 @@
+// C ABI: plan state, dimension validation, buffer sizing and pass dispatch.
+//
+// Host logic restated from the reference's FourierTransformer
+// (include/FastFFT.h:84-732, src/fastfft/FastFFT.cu:58-3379) with status codes in
+// place of std::abort().  The kernel sequence per call is chosen here:
+//   2D FwdFFT          r2c_rows (N_x, L_y rows)  -> cols FWD (N_y)
+//   2D InvFFT          cols INV (N_y, keep W_y)  -> c2r_rows (N_x, keep W_x)
+//   2D FwdImageInvFFT  r2c_rows -> cols XCORR (fwd, conj-mul, inv, keep W_y) -> c2r_rows
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "../../include/fastfft_capi.h"
+#include "kernels_2d.cuh"
+#include "launch.h"
+#include "plan.h"
+
+using namespace ffb;
+
+namespace {
+
+const char* kVersion = "fastfft_b200 0.1.0 (sm_100a)";
+
+thread_local std::string g_null_handle_error;
+
+fastfft_status fail(fastfft_plan_s* h, fastfft_status st, const std::string& msg) {
+    if (h)
+        h->last_error = msg;
+    else
+        g_null_handle_error = msg;
+    return st;
+}
+
+fastfft_status cuda_fail(fastfft_plan_s* h, cudaError_t e, const char* where) {
+    return fail(h, FASTFFT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+bool is_pow2(long long v) { return v >= 1 && (v & (v - 1)) == 0; }
+
+bool real_dtype(int d) { return d == FASTFFT_DTYPE_F32 || d == FASTFFT_DTYPE_F16 || d == FASTFFT_DTYPE_BF16; }
+bool cplx_dtype(int d) { return d == FASTFFT_DTYPE_C64 || d == FASTFFT_DTYPE_C32H || d == FASTFFT_DTYPE_C32BF; }
+
+size_t real_size(int d) { return d == FASTFFT_DTYPE_F32 ? 4 : 2; }
+
+long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+// ReturnPaddedMemorySize (include/FastFFT.h:363-404) for real-valued InputType.
+long long padded_elems(Dims& d) {
+    const int jump = (d.x % 2 == 0) ? 2 : 1;
+    d.w = (d.x + jump) / 2;
+    return 2LL * d.w * d.y * d.z;
+}
+
+// Classify one direction (FastFFT.cu:803-850).  Mixed growth/shrink is rejected.
+bool classify(const Dims& in, const Dims& out, SizeChange* sc, std::string* why) {
+    const bool any_up = out.x > in.x || out.y > in.y || out.z > in.z;
+    const bool any_down = out.x < in.x || out.y < in.y || out.z < in.z;
+    if (any_up && any_down) {
+        *why = "all dimensions must either increase, decrease or stay the same";
+        return false;
+    }
+    *sc = any_up ? SizeChange::Increase : any_down ? SizeChange::Decrease : SizeChange::NoChange;
+    return true;
+}
+
+fastfft_status validate(fastfft_plan_s* h) {
+    if (!h->fwd_set || !h->inv_set) return fail(h, FASTFFT_ERR_NOT_PLANNED, "forward and inverse plans must both be set");
+    if (h->validated) return FASTFFT_OK;
+    const Dims &fi = h->fwd_in, &fo = h->fwd_out, &ii = h->inv_in, &io = h->inv_out;
+    if (fo.x != ii.x || fo.y != ii.y || fo.z != ii.z)
+        return fail(h, FASTFFT_ERR_INVALID_DIMS, "forward output dims must match inverse input dims");
+    std::string why;
+    if (!classify(fi, fo, &h->fwd_change, &why)) return fail(h, FASTFFT_ERR_INVALID_DIMS, "forward plan: " + why);
+    if (!classify(ii, io, &h->inv_change, &why)) return fail(h, FASTFFT_ERR_INVALID_DIMS, "inverse plan: " + why);
+    // dimensionality (FastFFT.cu:866-890)
+    int dim;
+    if (fi.z == 1 && fo.z == 1) {
+        if (ii.z != 1 || io.z != 1)
+            return fail(h, FASTFFT_ERR_INVALID_DIMS, "fwd/inv dimensionality may not change (z dimension)");
+        if (fi.y == 1 && fo.y == 1) return fail(h, FASTFFT_ERR_UNSUPPORTED, "1D transforms are not supported");
+        dim = 2;
+    } else {
+        dim = 3;
+        const int m = 512;
+        const Dims* all[4] = {&fi, &fo, &ii, &io};
+        for (const Dims* d : all)
+            if (d->x > m || d->y > m || d->z > m)
+                return fail(h, FASTFFT_ERR_INVALID_DIMS, "all dimensions must be <= 512 for 3d transforms");
+    }
+    if (dim != h->rank) return fail(h, FASTFFT_ERR_INVALID_DIMS, "plan dimensionality does not match the handle rank");
+    // powers of two (FastFFT.cu:895-927)
+    if ((!is_pow2(fi.x) || !is_pow2(fi.y) || !is_pow2(fi.z)) && h->fwd_change != SizeChange::Increase)
+        return fail(h, FASTFFT_ERR_INVALID_DIMS, "input dimensions must be powers of 2 unless the forward transform pads");
+    if (!is_pow2(fo.x) || !is_pow2(fo.y) || !is_pow2(fo.z))
+        return fail(h, FASTFFT_ERR_INVALID_DIMS, "forward output dimensions must be powers of 2");
+    if ((!is_pow2(io.x) || !is_pow2(io.y) || !is_pow2(io.z)) && h->inv_change != SizeChange::Decrease)
+        return fail(h, FASTFFT_ERR_INVALID_DIMS, "output dimensions must be powers of 2 unless the inverse transform crops");
+    // transform sizes handled by the block FFTs
+    const long long nx = std::max(fi.x, fo.x), ny = std::max(fi.y, fo.y), nz = std::max(fi.z, fo.z);
+    auto in_range = [](long long n) { return n >= ffb::kMinN && n <= ffb::kMaxN; };
+    if (!in_range(nx) || !in_range(ny) || (dim == 3 && !in_range(nz)))
+        return fail(h, FASTFFT_ERR_UNSUPPORTED, "transform sizes must be in [16, 8192]");
+    if (!in_range(ii.x) || !in_range(ii.y)) return fail(h, FASTFFT_ERR_UNSUPPORTED, "transform sizes must be in [16, 8192]");
+    h->validated = true;
+    return FASTFFT_OK;
+}
+
+// Internal buffer layout (the reference's buffer_1 / buffer_2 pair):
+//   region A: [kx][y] forward row-pass output, pitch pA >= L_y (multiple of 4)
+//   region B: [kx][y] inverse column-pass output, pitch pB >= W_y (multiple of 4)
+void size_buffers(fastfft_plan_s* h) {
+    const long long nx_f = std::max(h->fwd_in.x, h->fwd_out.x);
+    h->pitch_a = round_up(h->fwd_in.y, 4);
+    const long long kx_f = nx_f / 2 + 1;
+    h->bytes_a = round_up(kx_f * h->pitch_a * 8, 256);
+    h->pitch_b = round_up(h->inv_out.y, 4);
+    const long long kx_i = h->inv_in.x / 2 + 1;
+    h->bytes_b = round_up(kx_i * h->pitch_b * 8, 256);
+}
+
+fastfft_status allocate(fastfft_plan_s* h) {
+    size_buffers(h);
+    const size_t need = (size_t)(h->bytes_a + h->bytes_b);
+    if (h->buffer && h->buffer_bytes >= need) return FASTFFT_OK;
+    if (h->buffer) {
+        cudaFree(h->buffer);
+        h->buffer = nullptr;
+        h->buffer_bytes = 0;
+    }
+    cudaError_t e = cudaGetDevice(&h->device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGetDevice");
+    // A plain (synchronous) allocation: the buffer is then valid on every stream the
+    // handle is later pointed at, not only on the stream that allocated it.
+    e = cudaMalloc(&h->buffer, need);
+    if (e != cudaSuccess) {
+        h->buffer = nullptr;
+        return fail(h, FASTFFT_ERR_ALLOC, std::string("cudaMalloc of the work buffer failed: ") + cudaGetErrorString(e));
+    }
+    h->buffer_bytes = need;
+    return FASTFFT_OK;
+}
+
+float scale_of(const fastfft_op* op) { return (op && op->kind == FASTFFT_OP_SCALE) ? op->scale : 1.f; }
+
+bool valid_op(const fastfft_op* op, bool intra) {
+    if (!op) return true;
+    if (intra) return op->kind == FASTFFT_OP_NOOP || op->kind == FASTFFT_OP_CONJ_MUL || op->kind == FASTFFT_OP_CONJ_MUL_THEN_SCALE;
+    return op->kind == FASTFFT_OP_NOOP || op->kind == FASTFFT_OP_SCALE;
+}
+
+fastfft_status prepare_call(fastfft_plan_s* h) {
+    fastfft_status st = validate(h);
+    if (st != FASTFFT_OK) return st;
+    if (!h->buffer) {
+        st = allocate(h);
+        if (st != FASTFFT_OK) return st;
+    }
+    if (h->rank != 2) return fail(h, FASTFFT_ERR_UNSUPPORTED, "3D transforms are not available in this build");
+    return FASTFFT_OK;
+}
+
+float2* region_a(fastfft_plan_s* h) { return static_cast<float2*>(h->buffer); }
+float2* region_b(fastfft_plan_s* h) { return reinterpret_cast<float2*>(static_cast<char*>(h->buffer) + h->bytes_a); }
+
+// Row pass of the forward transform into region A.
+fastfft_status run_fwd_rows(fastfft_plan_s* h, const void* in, float pre_scale, int kmax) {
+    const int nx = (int)std::max(h->fwd_in.x, h->fwd_out.x);
+    const float2* tw = nullptr;
+    cudaError_t e = twiddles_for(nx, &tw);
+    if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    RowFwdArgs a;
+    a.in = in;
+    a.in_pitch = 2LL * h->fwd_in.w;
+    a.n_rows = (int)h->fwd_in.y;
+    a.L = (int)h->fwd_in.x;
+    a.out = region_a(h);
+    a.out_pitch = h->pitch_a;
+    a.kmax = kmax;
+    a.scale = pre_scale;
+    a.tw = tw;
+    e = launch_r2c_rows(nx, h->input_dtype, a, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "r2c row pass");
+    return FASTFFT_OK;
+}
+
+fastfft_status run_inv_rows(fastfft_plan_s* h, void* out, float post_scale) {
+    const int nx = (int)h->inv_in.x;
+    const float2* tw = nullptr;
+    cudaError_t e = twiddles_for(nx, &tw);
+    if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    RowInvArgs a;
+    a.in = region_b(h);
+    a.in_pitch = h->pitch_b;
+    a.n_rows = (int)h->inv_out.y;
+    a.out = out;
+    a.out_pitch = 2LL * h->inv_out.w;
+    a.W = (int)h->inv_out.x;
+    a.scale = post_scale;
+    a.tw = tw;
+    e = launch_c2r_rows(nx, h->output_dtype, a, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "c2r row pass");
+    return FASTFFT_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+fastfft_status fastfft_create(fastfft_handle* out, int compute_dtype, int input_dtype, int image_dtype, int rank) {
+    if (!out) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle pointer");
+    *out = nullptr;
+    if (compute_dtype != FASTFFT_DTYPE_F32) return fail(nullptr, FASTFFT_ERR_UNSUPPORTED, "compute type must be float");
+    if (!real_dtype(input_dtype)) return fail(nullptr, FASTFFT_ERR_UNSUPPORTED, "input type must be a real type (f32, f16, bf16)");
+    if (!cplx_dtype(image_dtype)) return fail(nullptr, FASTFFT_ERR_UNSUPPORTED, "image type must be complex (c64, c32h, c32bf)");
+    if (rank != 2 && rank != 3) return fail(nullptr, FASTFFT_ERR_UNSUPPORTED, "only 2D and 3D FFTs are supported");
+    fastfft_plan_s* h = new (std::nothrow) fastfft_plan_s();
+    if (!h) return fail(nullptr, FASTFFT_ERR_ALLOC, "out of host memory");
+    h->compute_dtype = compute_dtype;
+    h->input_dtype = input_dtype;
+    h->output_dtype = input_dtype;
+    h->image_dtype = image_dtype;
+    h->rank = rank;
+    h->stream = cudaStreamPerThread;
+    *out = h;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_destroy(fastfft_handle h) {
+    if (!h) return FASTFFT_OK;
+    if (h->buffer) {
+        cudaStreamSynchronize(h->stream);
+        cudaFree(h->buffer);
+    }
+    delete h;
+    return FASTFFT_OK;
+}
+
+static fastfft_status set_plan(fastfft_handle h, bool fwd, size_t ix, size_t iy, size_t iz, size_t ox, size_t oy,
+                               size_t oz, int is_padded) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (ix == 0 || iy == 0 || iz == 0 || ox == 0 || oy == 0 || oz == 0)
+        return fail(h, FASTFFT_ERR_INVALID_DIMS, "logical dimensions must be > 0");
+    const size_t lim = 1u << 15;
+    if (ix >= lim || iy >= lim || iz >= lim || ox >= lim || oy >= lim || oz >= lim)
+        return fail(h, FASTFFT_ERR_INVALID_DIMS, "logical dimensions must be < 32768");
+    if (!is_padded) return fail(h, FASTFFT_ERR_UNSUPPORTED, "input arrays must be FFTW padded");
+    Dims in{(long long)ix, (long long)iy, (long long)iz, 0}, outd{(long long)ox, (long long)oy, (long long)oz, 0};
+    const long long n_in = padded_elems(in), n_out = padded_elems(outd);
+    if (fwd) {
+        h->fwd_in = in;
+        h->fwd_out = outd;
+        h->input_mem = n_in;
+        h->fwd_out_mem = n_out;
+        h->fwd_set = true;
+    } else {
+        h->inv_in = in;
+        h->inv_out = outd;
+        h->inv_out_mem = n_out;
+        h->inv_set = true;
+    }
+    h->compute_mem = std::max(h->compute_mem, std::max(n_in, n_out));
+    h->validated = false;
+    if (h->fwd_set && h->inv_set) {
+        fastfft_status st = validate(h);
+        if (st != FASTFFT_OK) return st;
+        size_buffers(h);
+        // AllocateBufferMemory happens on the second plan call, as in the reference.
+        // Without a visible CUDA device (host-only use of the plan logic) the
+        // allocation is deferred to the first transform, which then reports it.
+        int n_dev = 0;
+        if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {
+            cudaGetLastError();
+            return FASTFFT_OK;
+        }
+        return allocate(h);
+    }
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_set_forward_plan(fastfft_handle h, size_t ix, size_t iy, size_t iz, size_t ox, size_t oy,
+                                        size_t oz, int is_padded) {
+    return set_plan(h, true, ix, iy, iz, ox, oy, oz, is_padded);
+}
+
+fastfft_status fastfft_set_inverse_plan(fastfft_handle h, size_t ix, size_t iy, size_t iz, size_t ox, size_t oy,
+                                        size_t oz, int is_padded) {
+    return set_plan(h, false, ix, iy, iz, ox, oy, oz, is_padded);
+}
+
+fastfft_status fastfft_set_stream(fastfft_handle h, void* cuda_stream) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    h->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : cudaStreamPerThread;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_set_output_dtype(fastfft_handle h, int dtype) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (!real_dtype(dtype)) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "output dtype must be real (f32, f16, bf16)");
+    h->output_dtype = dtype;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_fwd(fastfft_handle h, const void* input, void* output, const fastfft_op* pre_op,
+                           const fastfft_op* intra_op) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (!input) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input pointer");
+    if (!valid_op(pre_op, false)) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "pre-op must be NOOP or SCALE");
+    if (intra_op && intra_op->kind != FASTFFT_OP_NOOP)
+        return fail(h, FASTFFT_ERR_UNSUPPORTED, "FwdFFT takes no intra-op (use FwdImageInvFFT)");
+    fastfft_status st = prepare_call(h);
+    if (st != FASTFFT_OK) return st;
+    void* out = output ? output : const_cast<void*>(input);
+    const int kmax = (int)h->fwd_out.w;
+    st = run_fwd_rows(h, input, scale_of(pre_op), kmax);
+    if (st != FASTFFT_OK) return st;
+    const int ny = (int)std::max(h->fwd_in.y, h->fwd_out.y);
+    const float2* tw = nullptr;
+    cudaError_t e = twiddles_for(ny, &tw);
+    if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    ColArgs c;
+    std::memset(&c, 0, sizeof(c));
+    c.in = region_a(h);
+    c.in_stride = h->pitch_a;
+    c.L = (int)h->fwd_in.y;
+    c.out = out;
+    c.out_stride = h->fwd_out.y;
+    c.W = (int)h->fwd_out.y;
+    c.n_cols = kmax;
+    c.in_scale = 1.f;
+    c.out_scale = 1.f;
+    c.intra_scale = 1.f;
+    c.tw = tw;
+    e = launch_cols_fwd(ny, c, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "forward column pass");
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_inv(fastfft_handle h, const void* input, void* output, const fastfft_op* intra_op,
+                           const fastfft_op* post_op) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (!input) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input pointer");
+    if (!valid_op(post_op, false)) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "post-op must be NOOP or SCALE");
+    if (intra_op && intra_op->kind != FASTFFT_OP_NOOP)
+        return fail(h, FASTFFT_ERR_UNSUPPORTED, "InvFFT takes no intra-op (use FwdImageInvFFT)");
+    fastfft_status st = prepare_call(h);
+    if (st != FASTFFT_OK) return st;
+    if (h->inv_change == SizeChange::Increase)
+        return fail(h, FASTFFT_ERR_UNSUPPORTED, "inverse size increase is not supported");
+    void* out = output ? output : const_cast<void*>(input);
+    const int ny = (int)h->inv_in.y;
+    const float2* tw = nullptr;
+    cudaError_t e = twiddles_for(ny, &tw);
+    if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    ColArgs c;
+    std::memset(&c, 0, sizeof(c));
+    c.in = input;
+    c.in_stride = h->inv_in.y;
+    c.L = (int)h->inv_in.y;
+    c.out = region_b(h);
+    c.out_stride = h->pitch_b;
+    c.W = (int)h->inv_out.y;
+    c.n_cols = (int)h->inv_in.w;
+    c.in_scale = 1.f;
+    c.out_scale = 1.f;
+    c.intra_scale = 1.f;
+    c.tw = tw;
+    e = launch_cols_inv(ny, c, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "inverse column pass");
+    return run_inv_rows(h, out, scale_of(post_op));
+}
+
+fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const void* image_spectrum, void* output,
+                                     const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                     const fastfft_op* post_op) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (!input || !image_spectrum) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image pointer");
+    if (!valid_op(pre_op, false)) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "pre-op must be NOOP or SCALE");
+    if (!valid_op(post_op, false)) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "post-op must be NOOP or SCALE");
+    if (!valid_op(intra_op, true))
+        return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "intra-op must be NOOP, CONJ_MUL or CONJ_MUL_THEN_SCALE");
+    fastfft_status st = prepare_call(h);
+    if (st != FASTFFT_OK) return st;
+    if (h->fwd_change == SizeChange::Decrease)
+        return fail(h, FASTFFT_ERR_UNSUPPORTED, "cross-correlation with a forward size decrease is not supported");
+    if (h->inv_change == SizeChange::Increase)
+        return fail(h, FASTFFT_ERR_UNSUPPORTED, "cross-correlation with an inverse size increase is not supported");
+    void* out = output ? output : const_cast<void*>(input);
+    const int nx = (int)h->fwd_out.x;
+    st = run_fwd_rows(h, input, scale_of(pre_op), nx / 2 + 1);
+    if (st != FASTFFT_OK) return st;
+    const int ny = (int)h->fwd_out.y;
+    const float2* tw = nullptr;
+    cudaError_t e = twiddles_for(ny, &tw);
+    if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    ColArgs c;
+    std::memset(&c, 0, sizeof(c));
+    c.in = region_a(h);
+    c.in_stride = h->pitch_a;
+    c.L = (int)h->fwd_in.y;
+    c.img = image_spectrum;
+    c.img_stride = ny;
+    c.out = region_b(h);
+    c.out_stride = h->pitch_b;
+    c.W = (int)h->inv_out.y;
+    c.n_cols = nx / 2 + 1;
+    c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
+    c.intra_scale = intra_op ? intra_op->scale : 1.f;
+    c.in_scale = 1.f;
+    c.out_scale = 1.f;
+    c.tw = tw;
+    e = launch_cols_xcorr(ny, h->image_dtype, c, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cross-correlation column pass");
+    return run_inv_rows(h, out, scale_of(post_op));
+}
+
+static fastfft_status get_ll(fastfft_handle h, long long* n, long long v) {
+    if (!h || !n) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null argument");
+    *n = v;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_input_memory_size(fastfft_handle h, long long* n) { return get_ll(h, n, h ? h->input_mem : 0); }
+fastfft_status fastfft_fwd_output_memory_size(fastfft_handle h, long long* n) {
+    return get_ll(h, n, h ? h->fwd_out_mem : 0);
+}
+fastfft_status fastfft_inv_output_memory_size(fastfft_handle h, long long* n) {
+    return get_ll(h, n, h ? h->inv_out_mem : 0);
+}
+fastfft_status fastfft_buffer_bytes(fastfft_handle h, long long* n) {
+    return get_ll(h, n, h ? (long long)h->buffer_bytes : 0);
+}
+
+static fastfft_status get_dims(fastfft_handle h, int dims[4], const Dims& d) {
+    if (!h || !dims) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null argument");
+    dims[0] = (int)d.x;
+    dims[1] = (int)d.y;
+    dims[2] = (int)d.z;
+    dims[3] = (int)d.w;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_fwd_input_dims(fastfft_handle h, int dims[4]) { return get_dims(h, dims, h ? h->fwd_in : Dims{}); }
+fastfft_status fastfft_fwd_output_dims(fastfft_handle h, int dims[4]) { return get_dims(h, dims, h ? h->fwd_out : Dims{}); }
+fastfft_status fastfft_inv_input_dims(fastfft_handle h, int dims[4]) { return get_dims(h, dims, h ? h->inv_in : Dims{}); }
+fastfft_status fastfft_inv_output_dims(fastfft_handle h, int dims[4]) { return get_dims(h, dims, h ? h->inv_out : Dims{}); }
+
+fastfft_status fastfft_wait(fastfft_handle h) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamSynchronize");
+    return FASTFFT_OK;
+}
+
+const char* fastfft_last_error(fastfft_handle h) { return h ? h->last_error.c_str() : g_null_handle_error.c_str(); }
+
+const char* fastfft_status_string(int status) {
+    switch (status) {
+        case FASTFFT_OK: return "ok";
+        case FASTFFT_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case FASTFFT_ERR_INVALID_DIMS: return "invalid dimensions";
+        case FASTFFT_ERR_UNSUPPORTED: return "unsupported";
+        case FASTFFT_ERR_NOT_PLANNED: return "not planned";
+        case FASTFFT_ERR_CUDA: return "cuda error";
+        case FASTFFT_ERR_ALLOC: return "allocation failed";
+        case FASTFFT_ERR_TIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+const char* fastfft_version(void) { return kVersion; }
+
+}  // extern "C"

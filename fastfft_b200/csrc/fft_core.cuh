@@ -1,0 +1,365 @@
+// Block FFT core for sm_100a: radix-16 register butterflies, Stockham passes with
+// shared-memory exchanges, FP64-generated twiddle tables.
+//
+// One length-N FFT (N = 2^m, 16 <= N <= 8192) is computed by T = N/16 threads.
+// Thread j holds v[q] = x[j + T*q] (q = 0..15) on entry and X[j + T*q] on exit, so
+// a column or row is read and written with unit stride across the threads.
+// The passes are: an optional first radix-REM pass (REM = N / 16^k in {2,4,8}, no
+// twiddles) followed by radix-16 passes with growing stride Ns; between passes the
+// values go through shared memory (one float2 of padding per 16 keeps the strided
+// writes free of bank conflicts).
+//
+// This replaces the cuFFTDx block FFT that the reference calls through
+// FFT().execute(thread_data, shared_mem, workspace) (e.g. src/fastfft/FastFFT.cu:42).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#ifndef FFB_PACKED_F32X2
+#define FFB_PACKED_F32X2 1
+#endif
+
+namespace ffb {
+
+constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
+
+// ---------------------------------------------------------------------------
+// Complex arithmetic on float2.  Component-aligned adds use the sm_100 paired
+// FP32 instructions (one instruction for both lanes of a complex number).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+#if FFB_PACKED_F32X2
+    return __fadd2_rn(a, b);
+#else
+    return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+#if FFB_PACKED_F32X2
+    return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+#else
+    return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
+
+__device__ __forceinline__ float2 cscale(float2 a, float s) {
+#if FFB_PACKED_F32X2
+    return __fmul2_rn(a, make_float2(s, s));
+#else
+    return make_float2(a.x * s, a.y * s);
+#endif
+}
+
+// a * w
+__device__ __forceinline__ float2 cmul(float2 a, float2 w) {
+    return make_float2(fmaf(a.x, w.x, -a.y * w.y), fmaf(a.x, w.y, a.y * w.x));
+}
+
+// a * conj(w)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 w) {
+    return make_float2(fmaf(a.x, w.x, a.y * w.y), fmaf(a.y, w.x, -a.x * w.y));
+}
+
+// conj(a) * b : the CONJ_MUL intra-op of the reference, (ax*bx + ay*by, ax*by - ay*bx)
+// (include/detail/functors.h:30-40).
+__device__ __forceinline__ float2 conj_mul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.x, b.y, -a.y * b.x));
+}
+
+// Multiplication by the constant roots of unity W16^m = exp(-+2 pi i m / 16).
+// Forward uses exp(-2 pi i m/16); inverse the conjugate.
+constexpr float kC1 = 0.923879532511286756128f;  // cos(pi/8)
+constexpr float kS1 = 0.382683432365089771728f;  // sin(pi/8)
+constexpr float kR2 = 0.707106781186547524401f;  // sqrt(2)/2
+
+template <bool INV, int M>
+__device__ __forceinline__ float2 mul_w16(float2 a) {
+    constexpr int m = M & 15;
+    if constexpr (m == 0) {
+        return a;
+    } else if constexpr (m == 4) {
+        // forward: -i ; inverse: +i
+        return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+    } else if constexpr (m == 8) {
+        return make_float2(-a.x, -a.y);
+    } else if constexpr (m == 12) {
+        return INV ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+    } else if constexpr (m == 2) {
+        // forward (1 - i)/sqrt2 ; inverse (1 + i)/sqrt2
+        return INV ? make_float2(kR2 * (a.x - a.y), kR2 * (a.x + a.y))
+                   : make_float2(kR2 * (a.x + a.y), kR2 * (a.y - a.x));
+    } else if constexpr (m == 6) {
+        // forward (-1 - i)/sqrt2 ; inverse (-1 + i)/sqrt2
+        return INV ? make_float2(-kR2 * (a.x + a.y), kR2 * (a.x - a.y))
+                   : make_float2(kR2 * (a.y - a.x), -kR2 * (a.x + a.y));
+    } else if constexpr (m == 10) {
+        return INV ? make_float2(kR2 * (a.y - a.x), -kR2 * (a.x + a.y))
+                   : make_float2(-kR2 * (a.x + a.y), kR2 * (a.x - a.y));
+    } else if constexpr (m == 14) {
+        return INV ? make_float2(kR2 * (a.x + a.y), kR2 * (a.y - a.x))
+                   : make_float2(kR2 * (a.x - a.y), kR2 * (a.x + a.y));
+    } else {
+        // general: angle m*pi/8
+        constexpr float c = (m == 1 || m == 15) ? kC1 : (m == 3 || m == 13) ? kS1 : (m == 5 || m == 11) ? -kS1 : -kC1;
+        constexpr float s = (m == 1 || m == 7) ? kS1 : (m == 3 || m == 5) ? kC1 : (m == 9 || m == 15) ? -kS1 : -kC1;
+        // exp(i*m*pi/8) = (c, s); forward multiplies by (c, -s)
+        return INV ? cmul(a, make_float2(c, s)) : cmul(a, make_float2(c, -s));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Small DFTs on registers (natural order in, natural order out)
+// ---------------------------------------------------------------------------
+template <bool INV>
+__device__ __forceinline__ void dft2(float2& a0, float2& a1) {
+    float2 t = csub(a0, a1);
+    a0 = cadd(a0, a1);
+    a1 = t;
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
+    float2 s0 = cadd(a0, a2), e = csub(a0, a2);
+    float2 s1 = cadd(a1, a3), d = csub(a1, a3);
+    a0 = cadd(s0, s1);
+    a2 = csub(s0, s1);
+    if (!INV) {
+        a1 = make_float2(e.x + d.y, e.y - d.x);
+        a3 = make_float2(e.x - d.y, e.y + d.x);
+    } else {
+        a1 = make_float2(e.x - d.y, e.y + d.x);
+        a3 = make_float2(e.x + d.y, e.y - d.x);
+    }
+}
+
+// DFT8 over v[B + S*r], r = 0..7.
+template <bool INV, int B, int S>
+__device__ __forceinline__ void dft8(float2 (&v)[16]) {
+    // n = n1 + 2 n2 ; first DFT4 over n2 for n1 = 0, 1
+    float2 a[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) a[r] = v[B + S * r];
+    dft4<INV>(a[0], a[2], a[4], a[6]);
+    dft4<INV>(a[1], a[3], a[5], a[7]);
+    // twiddles W8^(n1 k1) = W16^(2 n1 k1): n1 = 1, k1 = 1,2,3 at a[3], a[5], a[7]
+    a[3] = mul_w16<INV, 2>(a[3]);
+    a[5] = mul_w16<INV, 4>(a[5]);
+    a[7] = mul_w16<INV, 6>(a[7]);
+    // DFT2 over n1 for each k1: X[k1 + 4 k2]
+    dft2<INV>(a[0], a[1]);
+    dft2<INV>(a[2], a[3]);
+    dft2<INV>(a[4], a[5]);
+    dft2<INV>(a[6], a[7]);
+    // a[2 k1 + k2] holds X[k1 + 4 k2]
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++)
+#pragma unroll
+        for (int k2 = 0; k2 < 2; k2++) v[B + S * (k1 + 4 * k2)] = a[2 * k1 + k2];
+}
+
+// Twiddle stage inside the 4x4 decomposition of DFT16: a[n1 + 4 k1] *= W16^(n1 k1)
+template <bool INV>
+__device__ __forceinline__ void dft16_inner_twiddles(float2 (&a)[16]) {
+    a[5] = mul_w16<INV, 1>(a[5]);
+    a[9] = mul_w16<INV, 2>(a[9]);
+    a[13] = mul_w16<INV, 3>(a[13]);
+    a[6] = mul_w16<INV, 2>(a[6]);
+    a[10] = mul_w16<INV, 4>(a[10]);
+    a[14] = mul_w16<INV, 6>(a[14]);
+    a[7] = mul_w16<INV, 3>(a[7]);
+    a[11] = mul_w16<INV, 6>(a[11]);
+    a[15] = mul_w16<INV, 9>(a[15]);
+}
+
+// Final DFT4 over n1 and the 4x4 transpose back to natural order.
+template <bool INV>
+__device__ __forceinline__ void dft16_outer(float2 (&a)[16], float2 (&v)[16]) {
+    // a[n1 + 4 k1] after twiddles; DFT4 over n1 for each k1 -> X[k1 + 4 k2] at a[4 k1 + k2]
+    dft4<INV>(a[0], a[1], a[2], a[3]);
+    dft4<INV>(a[4], a[5], a[6], a[7]);
+    dft4<INV>(a[8], a[9], a[10], a[11]);
+    dft4<INV>(a[12], a[13], a[14], a[15]);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++)
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = a[4 * k1 + k2];
+}
+
+// Full DFT16 of v[0..15].
+template <bool INV>
+__device__ __forceinline__ void dft16(float2 (&v)[16]) {
+    // n = n1 + 4 n2: DFT4 over n2 for each n1 -> A[n1][k1] stored at a[n1 + 4 k1]
+    float2 a[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) a[i] = v[i];
+    dft4<INV>(a[0], a[4], a[8], a[12]);
+    dft4<INV>(a[1], a[5], a[9], a[13]);
+    dft4<INV>(a[2], a[6], a[10], a[14]);
+    dft4<INV>(a[3], a[7], a[11], a[15]);
+    dft16_inner_twiddles<INV>(a);
+    dft16_outer<INV>(a, v);
+}
+
+// DFT16 when only v[q], q < qnz, can be non-zero (forward size increase: the
+// zero-padded tail of a column is never loaded or transformed).
+template <bool INV>
+__device__ __forceinline__ void dft16_pruned(float2 (&v)[16], int qnz) {
+    if (qnz >= 16 || qnz > 8) {
+        dft16<INV>(v);
+        return;
+    }
+    if (qnz <= 1) {
+        float2 x0 = v[0];
+#pragma unroll
+        for (int k = 0; k < 16; k++) v[k] = x0;
+        return;
+    }
+    float2 a[16];
+    if (qnz <= 4) {
+        // n2 = 0 only: the first-stage DFT4s are copies
+#pragma unroll
+        for (int n1 = 0; n1 < 4; n1++) {
+            float2 x = v[n1];
+            a[n1] = x; a[n1 + 4] = x; a[n1 + 8] = x; a[n1 + 12] = x;
+        }
+    } else {
+        // n2 in {0, 1}: DFT4 of (x0, x1, 0, 0) = (x0 + x1, x0 -+ i x1, x0 - x1, x0 +- i x1)
+#pragma unroll
+        for (int n1 = 0; n1 < 4; n1++) {
+            float2 x0 = v[n1], x1 = v[n1 + 4];
+            a[n1] = cadd(x0, x1);
+            a[n1 + 8] = csub(x0, x1);
+            if (!INV) {
+                a[n1 + 4] = make_float2(x0.x + x1.y, x0.y - x1.x);
+                a[n1 + 12] = make_float2(x0.x - x1.y, x0.y + x1.x);
+            } else {
+                a[n1 + 4] = make_float2(x0.x - x1.y, x0.y + x1.x);
+                a[n1 + 12] = make_float2(x0.x + x1.y, x0.y - x1.x);
+            }
+        }
+    }
+    dft16_inner_twiddles<INV>(a);
+    dft16_outer<INV>(a, v);
+}
+
+// ---------------------------------------------------------------------------
+// Pass structure for one size
+// ---------------------------------------------------------------------------
+template <int N>
+struct FftShape {
+    static_assert(N >= 16 && N <= 8192 && (N & (N - 1)) == 0, "N must be a power of two in [16, 8192]");
+    static constexpr int LOG = ilog2(N);
+    static constexpr int T = N / 16;             // threads per FFT
+    static constexpr int REM = 1 << (LOG & 3);   // radix of the optional first pass
+    static constexpr int NP16 = LOG >> 2;        // number of radix-16 passes
+    static constexpr int SMEM = N + N / 16;      // float2 per FFT exchange buffer
+    // twiddle entries: for every radix-16 pass with stride Ns > 1, 16*Ns entries
+    static constexpr int tw_pass_offset(int p) {
+        int off = 0;
+        int ns = REM;
+        for (int i = 0; i < p; i++) {
+            if (ns > 1) off += 16 * ns;
+            ns *= 16;
+        }
+        return off;
+    }
+    static constexpr int TW_SIZE = tw_pass_offset(NP16);
+};
+
+// Offsets of each size's twiddle table inside the one device-wide table.
+constexpr int tw_size_of(int n) {
+    int log = ilog2(n), rem = 1 << (log & 3), np16 = log >> 2, off = 0, ns = rem;
+    for (int i = 0; i < np16; i++) {
+        if (ns > 1) off += 16 * ns;
+        ns *= 16;
+    }
+    return off;
+}
+constexpr int tw_base(int n) {
+    int off = 0;
+    for (int m = 16; m < n; m *= 2) off += tw_size_of(m);
+    return off;
+}
+constexpr int kMinN = 16;
+constexpr int kMaxN = 8192;
+constexpr int kTwTotal = tw_base(kMaxN) + tw_size_of(kMaxN);
+
+__device__ __forceinline__ int phys(int i) { return i + (i >> 4); }
+
+// Twiddle table layout for one size N, radix-16 pass with stride Ns:
+//   tw[off + r*Ns + t] = exp(-2 pi i r t / (16 Ns)),  r < 16, t < Ns.
+// Generated in FP64 (sincospi) and rounded to FP32 once.
+
+template <int N, bool INV>
+struct BlockFft {
+    using S = FftShape<N>;
+    static constexpr int T = S::T;
+
+    // Thread j of the FFT, v holds x[j + T q].  s: this FFT's exchange buffer
+    // (S::SMEM float2).  tw: the twiddle table for size N.  qnz: number of leading
+    // q slots that may be non-zero on input (16 = no pruning).
+    // All threads of the block must call this (it contains __syncthreads()).
+    __device__ __forceinline__ static void run(float2 (&v)[16], float2* __restrict__ s, int j,
+                                               const float2* __restrict__ tw, int qnz) {
+        if constexpr (S::REM > 1) {
+            constexpr int R = S::REM;
+            constexpr int M = 16 / R;
+            first_pass<R, M>(v);
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                const int b = j + T * m;
+#pragma unroll
+                for (int r = 0; r < R; r++) s[phys(b * R + r)] = v[m + r * M];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
+        }
+#pragma unroll
+        for (int p = 0; p < S::NP16; p++) {
+            const int ns = S::REM << (4 * p);
+            if (ns > 1) {
+                const float2* __restrict__ t = tw + S::tw_pass_offset(p) + (j & (ns - 1));
+#pragma unroll
+                for (int r = 1; r < 16; r++) {
+                    const float2 w = __ldg(t + r * ns);
+                    v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
+                }
+            }
+            if (S::REM == 1 && p == 0)
+                dft16_pruned<INV>(v, qnz);
+            else
+                dft16<INV>(v);
+            if (p < S::NP16 - 1) {
+                __syncthreads();
+                const int base = (j / ns) * 16 * ns + (j & (ns - 1));
+#pragma unroll
+                for (int r = 0; r < 16; r++) s[phys(base + r * ns)] = v[r];
+                __syncthreads();
+#pragma unroll
+                for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
+            }
+        }
+    }
+
+    template <int R, int M>
+    __device__ __forceinline__ static void first_pass(float2 (&v)[16]) {
+        if constexpr (R == 2) {
+#pragma unroll
+            for (int m = 0; m < M; m++) dft2<INV>(v[m], v[m + M]);
+        } else if constexpr (R == 4) {
+#pragma unroll
+            for (int m = 0; m < M; m++) dft4<INV>(v[m], v[m + M], v[m + 2 * M], v[m + 3 * M]);
+        } else if constexpr (R == 8) {
+            dft8<INV, 0, 2>(v);
+            dft8<INV, 1, 2>(v);
+        }
+    }
+};
+
+}  // namespace ffb

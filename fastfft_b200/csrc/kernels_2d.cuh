@@ -1,0 +1,281 @@
+// 2D passes of the size-changing FFT path (sm_100a).
+//
+//   r2c_rows   : row R2C along x of up to L_y rows, zero padding x >= L implicit,
+//                two real rows per complex FFT, output transposed to [kx][y]
+//                (replaces block_fft_kernel_R2C_{NONE,INCREASE,DECREASE}_XY,
+//                 src/fastfft/FastFFT.cu:1055-1077, :1107-1166, :1232-1261)
+//   cols       : column C2C along y over the [kx][y] layout; three modes
+//                  COL_FWD   forward, zero padding y >= L, keep first W outputs
+//                            (C2C_NONE / C2C_INCREASE / C2C_DECREASE, :1348-1475)
+//                  COL_INV   inverse, keep first W outputs (C2C inverse passes)
+//                  COL_XCORR forward (pruned) -> conj(T)*I intra-op against the
+//                            resident image spectrum -> inverse, keep first W
+//                            (the fused C2C_FWD_INCREASE_OP_INV_NONE, :20-56, extended
+//                             with the trimmed inverse that the reference aborts on,
+//                             :673-679)
+//   c2r_rows   : row C2R along x reading [kx][y], two rows per complex FFT, keep
+//                the first W_x outputs (C2R_NONE_XY / C2R_DECREASE_XY, :1641-1692)
+#pragma once
+
+#include "fft_core.cuh"
+
+namespace ffb {
+
+// ---------------------------------------------------------------------------
+// dtype helpers
+// ---------------------------------------------------------------------------
+template <class T> __device__ __forceinline__ float ld_real(const T* p);
+template <> __device__ __forceinline__ float ld_real<float>(const float* p) { return __ldg(p); }
+template <> __device__ __forceinline__ float ld_real<__half>(const __half* p) { return __half2float(__ldg(p)); }
+template <> __device__ __forceinline__ float ld_real<__nv_bfloat16>(const __nv_bfloat16* p) {
+    return __bfloat162float(__ldg(p));
+}
+
+template <class T> __device__ __forceinline__ void st_real(T* p, float v);
+template <> __device__ __forceinline__ void st_real<float>(float* p, float v) { *p = v; }
+template <> __device__ __forceinline__ void st_real<__half>(__half* p, float v) { *p = __float2half_rn(v); }
+template <> __device__ __forceinline__ void st_real<__nv_bfloat16>(__nv_bfloat16* p, float v) {
+    *p = __float2bfloat16_rn(v);
+}
+
+// Complex loads.  The streaming variant (evict-first) is used for the resident
+// image spectrum, which is read exactly once per template and should not push
+// the template's intermediates out of L2.
+template <class T> __device__ __forceinline__ float2 ld_cplx(const T* p);
+template <> __device__ __forceinline__ float2 ld_cplx<float2>(const float2* p) { return *p; }
+template <> __device__ __forceinline__ float2 ld_cplx<__half2>(const __half2* p) { return __half22float2(*p); }
+template <> __device__ __forceinline__ float2 ld_cplx<__nv_bfloat162>(const __nv_bfloat162* p) {
+    return __bfloat1622float2(*p);
+}
+
+template <class T> __device__ __forceinline__ float2 ld_cplx_stream(const T* p);
+template <> __device__ __forceinline__ float2 ld_cplx_stream<float2>(const float2* p) { return __ldcs(p); }
+template <> __device__ __forceinline__ float2 ld_cplx_stream<__half2>(const __half2* p) {
+    unsigned int u = __ldcs(reinterpret_cast<const unsigned int*>(p));
+    __half2 h = *reinterpret_cast<__half2*>(&u);
+    return __half22float2(h);
+}
+template <> __device__ __forceinline__ float2 ld_cplx_stream<__nv_bfloat162>(const __nv_bfloat162* p) {
+    unsigned int u = __ldcs(reinterpret_cast<const unsigned int*>(p));
+    __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162*>(&u);
+    return __bfloat1622float2(h);
+}
+
+// number of leading q slots (x[j + T q]) that can be non-zero when only n < L is loaded
+template <int T>
+__device__ __forceinline__ int leading_slots(int L, int j) {
+    if (L <= j) return 0;
+    int q = (L - j + T - 1) / T;
+    return q > 16 ? 16 : q;
+}
+
+// ---------------------------------------------------------------------------
+// Row R2C (forward), two rows per complex FFT
+// ---------------------------------------------------------------------------
+struct RowFwdArgs {
+    const void* in;        // real rows, row r at in + r * in_pitch (elements)
+    long long in_pitch;
+    int n_rows;            // rows that exist (rows >= n_rows are not produced)
+    int L;                 // valid x per row; x in [L, N) is zero padding
+    float2* out;           // out[k * out_pitch + r] for k < kmax
+    long long out_pitch;   // >= n_rows, even
+    int kmax;              // kx outputs written (N/2+1, or fewer for a decrease)
+    float scale;           // pre-op SCALE (1 = NOOP)
+    const float2* tw;      // twiddle table of size N
+};
+
+template <int N, class InT, int FPB>
+__global__ void __launch_bounds__(FftShape<N>::T * FPB)
+r2c_rows_kernel(RowFwdArgs a) {
+    using S = FftShape<N>;
+    constexpr int T = S::T;
+    extern __shared__ float2 smem[];
+    const int f = threadIdx.x / T;
+    const int j = threadIdx.x - f * T;
+    float2* s = smem + f * S::SMEM;
+    const int ra = 2 * (blockIdx.x * FPB + f);
+    const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
+    const InT* pa = static_cast<const InT*>(a.in) + (long long)ra * a.in_pitch;
+    const InT* pb = pa + a.in_pitch;
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int n = j + T * q;
+        float xa = 0.f, xb = 0.f;
+        if (n < a.L) {
+            if (has_a) xa = ld_real<InT>(pa + n);
+            if (has_b) xb = ld_real<InT>(pb + n);
+        }
+        v[q] = make_float2(xa * a.scale, xb * a.scale);
+    }
+    BlockFft<N, false>::run(v, s, j, a.tw, leading_slots<T>(a.L, j));
+
+    // Split Z = A + iB into the two real-row spectra: A[k] = (Z[k] + conj Z[N-k]) / 2,
+    // B[k] = -i (Z[k] - conj Z[N-k]) / 2.
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 16; q++) s[phys(j + T * q)] = v[q];
+    __syncthreads();
+    const int items = FPB * a.kmax;
+    for (int i = threadIdx.x; i < items; i += blockDim.x) {
+        const int ff = i % FPB;
+        const int k = i / FPB;
+        const float2* sf = smem + ff * S::SMEM;
+        const float2 z1 = sf[phys(k)];
+        const float2 z2 = sf[phys((N - k) & (N - 1))];
+        const float2 A = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
+        const float2 B = make_float2(0.5f * (z1.y + z2.y), 0.5f * (z2.x - z1.x));
+        const int rr = 2 * (blockIdx.x * FPB + ff);
+        float2* o = a.out + (long long)k * a.out_pitch + rr;
+        if (rr + 1 < a.n_rows) {
+            *reinterpret_cast<float4*>(o) = make_float4(A.x, A.y, B.x, B.y);
+        } else if (rr < a.n_rows) {
+            *o = A;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Column C2C
+// ---------------------------------------------------------------------------
+enum ColMode { COL_FWD = 0, COL_INV = 1, COL_XCORR = 2 };
+
+struct ColArgs {
+    const void* in;          // column c at in + c * in_stride (complex elements)
+    long long in_stride;
+    int L;                   // valid input rows per column (zero beyond)
+    const void* img;         // XCORR: image spectrum column c at img + c * img_stride
+    long long img_stride;
+    void* out;               // column c at out + c * out_stride
+    long long out_stride;
+    int W;                   // outputs kept per column
+    int n_cols;
+    int intra_kind;          // 0 NOOP, 2 CONJ_MUL, 3 CONJ_MUL_THEN_SCALE
+    float intra_scale;
+    float in_scale;
+    float out_scale;
+    const float2* tw;
+};
+
+template <int N, int MODE, class InC, class ImgC, class OutC, int FPB>
+__global__ void __launch_bounds__(FftShape<N>::T * FPB, (FftShape<N>::T * FPB <= 256) ? 2 : 1)
+cols_kernel(ColArgs a) {
+    using S = FftShape<N>;
+    constexpr int T = S::T;
+    extern __shared__ float2 smem[];
+    const int f = threadIdx.x / T;
+    const int j = threadIdx.x - f * T;
+    float2* s = smem + f * S::SMEM;
+    const int col = blockIdx.x * FPB + f;
+    const bool valid = col < a.n_cols;
+    const InC* pin = static_cast<const InC*>(a.in) + (long long)col * a.in_stride;
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int n = j + T * q;
+        float2 x = make_float2(0.f, 0.f);
+        if (valid && n < a.L) x = ld_cplx<InC>(pin + n);
+        v[q] = (a.in_scale != 1.f) ? cscale(x, a.in_scale) : x;
+    }
+    const int qnz = valid ? leading_slots<T>(a.L, j) : 0;
+    if constexpr (MODE == COL_INV) {
+        BlockFft<N, true>::run(v, s, j, a.tw, qnz);
+    } else {
+        BlockFft<N, false>::run(v, s, j, a.tw, qnz);
+    }
+    if constexpr (MODE == COL_XCORR) {
+        if (a.intra_kind != 0) {
+            const ImgC* pimg = static_cast<const ImgC*>(a.img) + (long long)col * a.img_stride;
+            const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                float2 im = make_float2(0.f, 0.f);
+                if (valid) im = ld_cplx_stream<ImgC>(pimg + j + T * q);
+                float2 p = conj_mul(v[q], im);
+                v[q] = (sc != 1.f) ? cscale(p, sc) : p;
+            }
+        }
+        BlockFft<N, true>::run(v, s, j, a.tw, 16);
+    }
+    if (valid) {
+        OutC* pout = static_cast<OutC*>(a.out) + (long long)col * a.out_stride;
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int n = j + T * q;
+            if (n < a.W) {
+                float2 x = (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q];
+                pout[n] = x;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row C2R (inverse), two rows per complex FFT
+// ---------------------------------------------------------------------------
+struct RowInvArgs {
+    const float2* in;      // in[k * in_pitch + r], k in [0, N/2], r < n_rows
+    long long in_pitch;    // even
+    int n_rows;
+    void* out;             // real rows, row r at out + r * out_pitch (elements)
+    long long out_pitch;
+    int W;                 // x outputs kept per row
+    float scale;           // post-op SCALE (1 = NOOP)
+    const float2* tw;
+};
+
+template <int N, class OutT, int FPB>
+__global__ void __launch_bounds__(FftShape<N>::T * FPB)
+c2r_rows_kernel(RowInvArgs a) {
+    using S = FftShape<N>;
+    constexpr int T = S::T;
+    constexpr int H = N / 2;
+    extern __shared__ float2 smem[];
+    const int f = threadIdx.x / T;
+    const int j = threadIdx.x - f * T;
+    float2* s = smem + f * S::SMEM;
+    // Gather rows (2 per FFT) and build Z[k] = A[k] + i B[k] over the full circle
+    // from the half spectrum (A, B Hermitian).  The imaginary parts of the k = 0
+    // and k = N/2 bins are dropped, as a C2R of a Hermitian spectrum does.
+    const int items = FPB * (H + 1);
+    for (int i = threadIdx.x; i < items; i += blockDim.x) {
+        const int ff = i % FPB;
+        const int k = i / FPB;
+        const int rr = 2 * (blockIdx.x * FPB + ff);
+        float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
+        const float2* p = a.in + (long long)k * a.in_pitch + rr;
+        if (rr + 1 < a.n_rows) {
+            const float4 t = *reinterpret_cast<const float4*>(p);
+            A = make_float2(t.x, t.y);
+            B = make_float2(t.z, t.w);
+        } else if (rr < a.n_rows) {
+            A = *p;
+        }
+        float2* sf = smem + ff * S::SMEM;
+        if (k == 0 || k == H) {
+            sf[phys(k)] = make_float2(A.x, B.x);
+        } else {
+            sf[phys(k)] = make_float2(A.x - B.y, A.y + B.x);
+            sf[phys(N - k)] = make_float2(A.x + B.y, B.x - A.y);
+        }
+    }
+    __syncthreads();
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
+    BlockFft<N, true>::run(v, s, j, a.tw, 16);
+    const int ra = 2 * (blockIdx.x * FPB + f);
+    OutT* oa = static_cast<OutT*>(a.out) + (long long)ra * a.out_pitch;
+    OutT* ob = oa + a.out_pitch;
+    const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int n = j + T * q;
+        if (n < a.W) {
+            if (has_a) st_real<OutT>(oa + n, v[q].x * a.scale);
+            if (has_b) st_real<OutT>(ob + n, v[q].y * a.scale);
+        }
+    }
+}
+
+}  // namespace ffb

@@ -1,0 +1,29 @@
+// Host-side launchers for the pass kernels (one translation unit per kernel family,
+// so the sm_100a build compiles in parallel).  Each launcher picks the compile-time
+// FFT size from the runtime N (power of two in [16, 8192]) and the data types.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+
+namespace ffb {
+
+struct RowFwdArgs;
+struct ColArgs;
+struct RowInvArgs;
+
+// dtype codes follow fastfft_dtype in include/fastfft_capi.h
+cudaError_t launch_r2c_rows(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
+cudaError_t launch_c2r_rows(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
+cudaError_t launch_cols_fwd(int n, const ColArgs& a, cudaStream_t st);
+cudaError_t launch_cols_inv(int n, const ColArgs& a, cudaStream_t st);
+cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st);
+
+// Device-wide FP64-generated twiddle table (generated once per device).
+cudaError_t twiddles_for(int n, const float2** out);
+
+// Sets cudaFuncAttributeMaxDynamicSharedMemorySize once per (kernel, device).
+cudaError_t ensure_smem_attr(const void* func, size_t bytes, std::atomic<unsigned long long>* done_mask);
+
+}  // namespace ffb

@@ -1,0 +1,64 @@
+// Launchers for the row passes (R2C forward, C2R inverse).
+#include "launch_common.cuh"
+
+namespace ffb {
+
+template <int N, class InT>
+static cudaError_t r2c_impl(const RowFwdArgs& a, cudaStream_t st) {
+    constexpr int FPB = row_fpb<N>();
+    constexpr int THREADS = FftShape<N>::T * FPB;
+    const size_t smem = (size_t)FPB * FftShape<N>::SMEM * sizeof(float2);
+    static std::atomic<unsigned long long> mask{0};
+    auto fn = r2c_rows_kernel<N, InT, FPB>;
+    cudaError_t e = ensure_smem_attr((const void*)fn, smem, &mask);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.n_rows + 2 * FPB - 1) / (2 * FPB);
+    if (grid == 0) return cudaSuccess;
+    fn<<<grid, THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int N>
+static cudaError_t r2c_dispatch(int in_dtype, const RowFwdArgs& a, cudaStream_t st) {
+    switch (in_dtype) {
+        case 0: return r2c_impl<N, float>(a, st);
+        case 1: return r2c_impl<N, __half>(a, st);
+        case 2: return r2c_impl<N, __nv_bfloat16>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_r2c_rows(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st) {
+    FFB_SIZE_SWITCH(n, r2c_dispatch, in_dtype, a, st)
+}
+
+template <int N, class OutT>
+static cudaError_t c2r_impl(const RowInvArgs& a, cudaStream_t st) {
+    constexpr int FPB = row_fpb<N>();
+    constexpr int THREADS = FftShape<N>::T * FPB;
+    const size_t smem = (size_t)FPB * FftShape<N>::SMEM * sizeof(float2);
+    static std::atomic<unsigned long long> mask{0};
+    auto fn = c2r_rows_kernel<N, OutT, FPB>;
+    cudaError_t e = ensure_smem_attr((const void*)fn, smem, &mask);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.n_rows + 2 * FPB - 1) / (2 * FPB);
+    if (grid == 0) return cudaSuccess;
+    fn<<<grid, THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int N>
+static cudaError_t c2r_dispatch(int out_dtype, const RowInvArgs& a, cudaStream_t st) {
+    switch (out_dtype) {
+        case 0: return c2r_impl<N, float>(a, st);
+        case 1: return c2r_impl<N, __half>(a, st);
+        case 2: return c2r_impl<N, __nv_bfloat16>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_c2r_rows(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st) {
+    FFB_SIZE_SWITCH(n, c2r_dispatch, out_dtype, a, st)
+}
+
+}  // namespace ffb

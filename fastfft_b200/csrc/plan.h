@@ -1,0 +1,46 @@
+// Plan state behind a fastfft_handle (the reference keeps the same state as members of
+// FourierTransformer, include/FastFFT.h:319-362 and :680-732).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+
+namespace ffb {
+
+struct Dims {
+    long long x = 0, y = 0, z = 0;
+    long long w = 0;  // complex elements along x after an R2C (ReturnPaddedMemorySize)
+};
+
+enum class SizeChange { Increase = 0, Decrease = 1, NoChange = 2 };
+
+}  // namespace ffb
+
+struct fastfft_plan_s {
+    int compute_dtype = 0;
+    int input_dtype = 0;
+    int output_dtype = 0;
+    int image_dtype = 3;
+    int rank = 2;
+    int device = 0;
+
+    ffb::Dims fwd_in, fwd_out, inv_in, inv_out;
+    bool fwd_set = false, inv_set = false, validated = false;
+    ffb::SizeChange fwd_change = ffb::SizeChange::NoChange;
+    ffb::SizeChange inv_change = ffb::SizeChange::NoChange;
+
+    // ReturnInputMemorySize / ReturnFwdOutputMemorySize / ReturnInvOutputMemorySize and
+    // compute_memory_wanted_ (element counts, include/FastFFT.h:194-204, :363-404)
+    long long input_mem = 0, fwd_out_mem = 0, inv_out_mem = 0, compute_mem = 0;
+
+    // work buffer: region A (forward row-pass output) then region B (inverse
+    // column-pass output); pitches in complex elements
+    void* buffer = nullptr;
+    size_t buffer_bytes = 0;
+    long long pitch_a = 0, bytes_a = 0, pitch_b = 0, bytes_b = 0;
+
+    cudaStream_t stream = cudaStreamPerThread;
+    std::string last_error;
+};

@@ -1,0 +1,96 @@
+// Device-wide twiddle table and per-device/per-kernel one-time set-up.
+#include <mutex>
+
+#include "launch_common.cuh"
+
+namespace ffb {
+
+// ---------------------------------------------------------------------------
+// Twiddle table generation: FP64 sincospi, rounded once to FP32
+// ---------------------------------------------------------------------------
+static __global__ void init_twiddles_kernel(float2* tw) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= kTwTotal) return;
+    // locate (size n, pass stride ns, r, t) of entry gid
+    int base = 0;
+    for (int n = kMinN; n <= kMaxN; n *= 2) {
+        const int sz = tw_size_of(n);
+        if (gid < base + sz) {
+            int local = gid - base;
+            const int log = ilog2(n);
+            int ns = 1 << (log & 3);
+            const int np16 = log >> 2;
+            for (int p = 0; p < np16; p++) {
+                if (ns > 1) {
+                    if (local < 16 * ns) {
+                        const int r = local / ns;
+                        const int t = local - r * ns;
+                        // exp(-2 pi i r t / (16 ns)) = cospi(-x) + i sinpi(-x), x = r t / (8 ns)
+                        const double x = -(double)(r * t) / (double)(8 * ns);
+                        double sv, cv;
+                        sincospi(x, &sv, &cv);
+                        tw[gid] = make_float2((float)cv, (float)sv);
+                        return;
+                    }
+                    local -= 16 * ns;
+                }
+                ns *= 16;
+            }
+            return;
+        }
+        base += sz;
+    }
+}
+
+
+// One table for every supported size, generated on the device in FP64 and rounded
+// once to FP32 (the reference evaluates __sincosf per element instead,
+// include/detail/device_functions.h:17-27).
+__device__ float2 g_twiddles[kTwTotal];
+
+namespace {
+std::mutex g_tw_mutex;
+const float2* g_tw_ptr[64] = {nullptr};
+}  // namespace
+
+cudaError_t twiddles_for(int n, const float2** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_tw_mutex);
+    if (!g_tw_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_twiddles);
+        if (e != cudaSuccess) return e;
+        cudaStream_t s;
+        e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+        init_twiddles_kernel<<<(kTwTotal + 255) / 256, 256, 0, s>>>(static_cast<float2*>(p));
+        e = cudaGetLastError();
+        cudaError_t e2 = cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        if (e != cudaSuccess) return e;
+        if (e2 != cudaSuccess) return e2;
+        g_tw_ptr[dev] = static_cast<const float2*>(p);
+    }
+    int base = 0;
+    for (int m = kMinN; m < n; m *= 2) base += tw_size_of(m);
+    *out = g_tw_ptr[dev] + base;
+    return cudaSuccess;
+}
+
+cudaError_t ensure_smem_attr(const void* func, size_t bytes, std::atomic<unsigned long long>* done_mask) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done_mask->load(std::memory_order_acquire) & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    done_mask->fetch_or(bit, std::memory_order_acq_rel);
+    return cudaSuccess;
+}
+
+}  // namespace ffb

@@ -1,0 +1,168 @@
+"""Python mirror of FastFFT::FourierTransformer over the C ABI.
+
+Method names, argument order and meaning follow the reference class
+(include/FastFFT.h:84-219): SetForwardFFTPlan / SetInverseFFTPlan, FwdFFT, InvFFT,
+FwdImageInvFFT, Return*MemorySize, Return*Dimensions, Wait.  Buffers are device
+pointers: torch CUDA tensors or raw integer addresses.  Where the reference calls
+std::abort() on a user error, this class raises FastFFTError with the library's
+message.
+
+Work is queued on torch's current CUDA stream unless a stream was set explicitly
+with SetStream (the reference always uses cudaStreamPerThread, usage.md:13).
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _capi as C
+
+_REAL_DTYPES = {"float32": C.DTYPE_F32, "float16": C.DTYPE_F16, "bfloat16": C.DTYPE_BF16}
+_CPLX_DTYPES = {"complex64": C.DTYPE_C64, "complex32": C.DTYPE_C32H, "chalf": C.DTYPE_C32H,
+                "complex_bf16": C.DTYPE_C32BF}
+
+
+def _dtype_code(name, table):
+    name = str(name).replace("torch.", "")
+    if name not in table:
+        raise ValueError(f"unsupported dtype {name}; expected one of {sorted(table)}")
+    return table[name]
+
+
+class KernelFunction:
+    """Functor descriptors, mirroring KernelFunction::my_functor (include/detail/functors.h)."""
+
+    @staticmethod
+    def noop():
+        return C.fastfft_op(C.OP_NOOP, 1.0)
+
+    @staticmethod
+    def scale(s: float):
+        return C.fastfft_op(C.OP_SCALE, float(s))
+
+    @staticmethod
+    def conj_mul():
+        return C.fastfft_op(C.OP_CONJ_MUL, 1.0)
+
+    @staticmethod
+    def conj_mul_then_scale(s: float):
+        return C.fastfft_op(C.OP_CONJ_MUL_THEN_SCALE, float(s))
+
+
+def _ptr(x) -> int | None:
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if hasattr(x, "is_cuda") and not x.is_cuda:
+            raise ValueError("FastFFT buffers must be CUDA device memory")
+        return x.data_ptr()
+    raise TypeError(f"cannot take a device pointer of {type(x)}")
+
+
+def _opref(op):
+    return ctypes.byref(op) if op is not None else None
+
+
+class FourierTransformer:
+    def __init__(self, compute_dtype="float32", input_dtype="float32", image_dtype="complex64", rank=2):
+        self._lib = C.lib()
+        self._h = C.Handle()
+        st = self._lib.fastfft_create(ctypes.byref(self._h), _dtype_code(compute_dtype, {"float32": 0}),
+                                      _dtype_code(input_dtype, _REAL_DTYPES),
+                                      _dtype_code(image_dtype, _CPLX_DTYPES), int(rank))
+        if st != C.OK:
+            raise C.FastFFTError(st, self._lib.fastfft_last_error(None).decode())
+        self._stream = None
+        self.rank = rank
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.fastfft_destroy(h)
+            self._h = C.Handle()
+
+    # -- helpers ---------------------------------------------------------
+    def _check(self, st):
+        if st != C.OK:
+            raise C.FastFFTError(st, self._lib.fastfft_last_error(self._h).decode())
+
+    def _bind_stream(self):
+        if self._stream is not None:
+            return
+        try:
+            import torch
+        except ImportError:  # pragma: no cover - torch is part of the image
+            return
+        if torch.cuda.is_available():
+            self._check(self._lib.fastfft_set_stream(self._h, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+    # -- plans -----------------------------------------------------------
+    def SetForwardFFTPlan(self, ix, iy, iz, ox, oy, oz, is_padded_output=True):
+        self._check(self._lib.fastfft_set_forward_plan(self._h, ix, iy, iz, ox, oy, oz, int(bool(is_padded_output))))
+
+    def SetInverseFFTPlan(self, ix, iy, iz, ox, oy, oz, is_padded_output=True):
+        self._check(self._lib.fastfft_set_inverse_plan(self._h, ix, iy, iz, ox, oy, oz, int(bool(is_padded_output))))
+
+    def SetStream(self, stream):
+        """Fix the work stream (a torch.cuda.Stream, a raw cudaStream_t, or None for cudaStreamPerThread)."""
+        raw = getattr(stream, "cuda_stream", stream)
+        self._stream = stream if stream is not None else 0
+        self._check(self._lib.fastfft_set_stream(self._h, ctypes.c_void_p(raw) if raw else None))
+
+    def SetOutputDtype(self, dtype):
+        self._check(self._lib.fastfft_set_output_dtype(self._h, _dtype_code(dtype, _REAL_DTYPES)))
+
+    # -- transforms ------------------------------------------------------
+    def FwdFFT(self, input_ptr, output_ptr=None, pre_op=None, intra_op=None):
+        self._bind_stream()
+        self._check(self._lib.fastfft_fwd(self._h, _ptr(input_ptr), _ptr(output_ptr), _opref(pre_op), _opref(intra_op)))
+
+    def InvFFT(self, input_ptr, output_ptr=None, intra_op=None, post_op=None):
+        self._bind_stream()
+        self._check(self._lib.fastfft_inv(self._h, _ptr(input_ptr), _ptr(output_ptr), _opref(intra_op), _opref(post_op)))
+
+    def FwdImageInvFFT(self, input_ptr, image_to_search, output_ptr=None, pre_op=None, intra_op=None, post_op=None):
+        if intra_op is None:
+            intra_op = KernelFunction.conj_mul()
+        self._bind_stream()
+        self._check(self._lib.fastfft_fwd_image_inv(self._h, _ptr(input_ptr), _ptr(image_to_search), _ptr(output_ptr),
+                                                    _opref(pre_op), _opref(intra_op), _opref(post_op)))
+
+    def Wait(self):
+        self._check(self._lib.fastfft_wait(self._h))
+
+    # -- queries ---------------------------------------------------------
+    def _ll(self, fn):
+        v = ctypes.c_longlong()
+        self._check(fn(self._h, ctypes.byref(v)))
+        return v.value
+
+    def ReturnInputMemorySize(self):
+        return self._ll(self._lib.fastfft_input_memory_size)
+
+    def ReturnFwdOutputMemorySize(self):
+        return self._ll(self._lib.fastfft_fwd_output_memory_size)
+
+    def ReturnInvOutputMemorySize(self):
+        return self._ll(self._lib.fastfft_inv_output_memory_size)
+
+    def ReturnBufferBytes(self):
+        return self._ll(self._lib.fastfft_buffer_bytes)
+
+    def _dims(self, fn):
+        d = (ctypes.c_int * 4)()
+        self._check(fn(self._h, d))
+        return tuple(d)
+
+    def ReturnFwdInputDimensions(self):
+        return self._dims(self._lib.fastfft_fwd_input_dims)
+
+    def ReturnFwdOutputDimensions(self):
+        return self._dims(self._lib.fastfft_fwd_output_dims)
+
+    def ReturnInvInputDimensions(self):
+        return self._dims(self._lib.fastfft_inv_input_dims)
+
+    def ReturnInvOutputDimensions(self):
+        return self._dims(self._lib.fastfft_inv_output_dims)

@@ -1,0 +1,135 @@
+/*
+ * fastfft_capi.h -- C ABI of the B200-native size-changing FFT library
+ * (libfastfft_b200.so).  Plain pointers, sizes and integer codes only.
+ *
+ * Every entry point below replaces one piece of the reference's
+ * FastFFT::FourierTransformer<ComputeBaseType, InputType, OtherImageType, Rank>
+ * (reference: include/FastFFT.h:84-219, src/fastfft/FastFFT.cu:58-3379) and is what a
+ * ctypes / cgo / JNI binding of that path would call.  The reference aborts on
+ * user error (include/detail/checks_and_debug.h:86-87); here every call returns a
+ * fastfft_status and the message of the last failure is kept per handle.
+ *
+ * Conventions (identical to the reference):
+ *   - dims are logical (x, y, z); z = 1 for 2D.
+ *   - real arrays use the FFTW pitch 2*(x/2+1) elements per row.
+ *   - spectra are complex64 in the transposed layout [kz][kx][ky], ky contiguous,
+ *     kx in [0, Nx/2]; for 2D that is [kx][ky].
+ *   - forward sign -1, no normalisation (a round trip scales by Nx*Ny*Nz).
+ *   - size decrease keeps the first outputs along each axis (window at the origin).
+ *   - all work is asynchronous on the handle's stream (default cudaStreamPerThread).
+ *   - an output pointer of NULL means "in place" (written over the input buffer,
+ *     which must then hold the larger of the two sizes).
+ */
+#ifndef FASTFFT_B200_CAPI_H
+#define FASTFFT_B200_CAPI_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define FASTFFT_API __attribute__((visibility("default")))
+#else
+#define FASTFFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fastfft_plan_s* fastfft_handle;
+
+typedef enum {
+    FASTFFT_OK = 0,
+    FASTFFT_ERR_INVALID_ARGUMENT = 1, /* null handle/pointer, bad dtype or op            */
+    FASTFFT_ERR_INVALID_DIMS = 2,     /* dimension rules of ValidateDimensions violated  */
+    FASTFFT_ERR_UNSUPPORTED = 3,      /* valid request that this library does not do     */
+    FASTFFT_ERR_NOT_PLANNED = 4,      /* transform called before both plans were set    */
+    FASTFFT_ERR_CUDA = 5,             /* a CUDA runtime call failed                      */
+    FASTFFT_ERR_ALLOC = 6,            /* device allocation failed                        */
+    FASTFFT_ERR_TIMEOUT = 7           /* a bounded device wait gave up                   */
+} fastfft_status;
+
+typedef enum {
+    FASTFFT_DTYPE_F32 = 0,  /* float            (real)    */
+    FASTFFT_DTYPE_F16 = 1,  /* __half           (real)    */
+    FASTFFT_DTYPE_BF16 = 2, /* __nv_bfloat16    (real)    */
+    FASTFFT_DTYPE_C64 = 3,  /* float2           (complex) */
+    FASTFFT_DTYPE_C32H = 4, /* __half2          (complex) */
+    FASTFFT_DTYPE_C32BF = 5 /* __nv_bfloat162   (complex) */
+} fastfft_dtype;
+
+/* Functor kinds, mirroring KernelFunction::my_functor (include/detail/functors.h:15-80). */
+typedef enum {
+    FASTFFT_OP_NOOP = 0,
+    FASTFFT_OP_SCALE = 1,              /* x * scale (pre-op / post-op)                      */
+    FASTFFT_OP_CONJ_MUL = 2,           /* conj(template) * image   (intra-op)              */
+    FASTFFT_OP_CONJ_MUL_THEN_SCALE = 3 /* conj(template) * image * scale (intra-op)        */
+} fastfft_op_kind;
+
+typedef struct {
+    int kind;    /* fastfft_op_kind */
+    float scale; /* used by SCALE and CONJ_MUL_THEN_SCALE */
+} fastfft_op;
+
+/* FourierTransformer() constructor (FastFFT.cu:58-74).  compute_dtype must be F32;
+ * input_dtype F32/F16/BF16 (real data; the reference's InputType); image_dtype
+ * C64/C32H/C32BF (OtherImageType); rank 2 or 3. */
+FASTFFT_API fastfft_status fastfft_create(fastfft_handle* out, int compute_dtype, int input_dtype, int image_dtype,
+                              int rank);
+/* ~FourierTransformer() (FastFFT.cu:76-80, Deallocate :105-113). */
+FASTFFT_API fastfft_status fastfft_destroy(fastfft_handle h);
+
+/* SetForwardFFTPlan (FastFFT.cu:132-161).  is_padded must be 1 (the reference asserts it). */
+FASTFFT_API fastfft_status fastfft_set_forward_plan(fastfft_handle h, size_t ix, size_t iy, size_t iz, size_t ox, size_t oy,
+                                        size_t oz, int is_padded);
+/* SetInverseFFTPlan (FastFFT.cu:180-200); the second of the two allocates the buffer
+ * (AllocateBufferMemory, FastFFT.cu:210-227). */
+FASTFFT_API fastfft_status fastfft_set_inverse_plan(fastfft_handle h, size_t ix, size_t iy, size_t iz, size_t ox, size_t oy,
+                                        size_t oz, int is_padded);
+
+/* Work stream; NULL selects cudaStreamPerThread (the reference's only stream, usage.md:13). */
+FASTFFT_API fastfft_status fastfft_set_stream(fastfft_handle h, void* cuda_stream);
+/* Real output dtype of InvFFT / FwdImageInvFFT (default: input_dtype, as in the reference). */
+FASTFFT_API fastfft_status fastfft_set_output_dtype(fastfft_handle h, int dtype);
+
+/* FwdFFT(input, output, pre_op, intra_op) (FastFFT.h:165-170, FastFFT.cu:263-277).
+ * Ops may be NULL (NOOP).  Output: complex64 spectrum [kz][kx][ky]. */
+FASTFFT_API fastfft_status fastfft_fwd(fastfft_handle h, const void* input, void* output, const fastfft_op* pre_op,
+                           const fastfft_op* intra_op);
+/* InvFFT(input, output, intra_op, post_op) (FastFFT.h:172-177, FastFFT.cu:279-293). */
+FASTFFT_API fastfft_status fastfft_inv(fastfft_handle h, const void* input, void* output, const fastfft_op* intra_op,
+                           const fastfft_op* post_op);
+/* FwdImageInvFFT(input, image_to_search, output, pre_op, intra_op, post_op)
+ * (FastFFT.h:179-187, FastFFT.cu:295-313, Generic_Fwd_Image_Inv :609-798).
+ * image_spectrum has the forward output's layout and the handle's image_dtype. */
+FASTFFT_API fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const void* image_spectrum, void* output,
+                                     const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                     const fastfft_op* post_op);
+
+/* ReturnInputMemorySize / ReturnFwdOutputMemorySize / ReturnInvOutputMemorySize
+ * (FastFFT.h:194-204): element counts of InputType, FFTW-padded. */
+FASTFFT_API fastfft_status fastfft_input_memory_size(fastfft_handle h, long long* n);
+FASTFFT_API fastfft_status fastfft_fwd_output_memory_size(fastfft_handle h, long long* n);
+FASTFFT_API fastfft_status fastfft_inv_output_memory_size(fastfft_handle h, long long* n);
+/* Return{Fwd,Inv}{Input,Output}Dimensions (FastFFT.h:206-220): {x, y, z, w}, w = complex
+ * elements along x after the R2C (set by ReturnPaddedMemorySize, FastFFT.h:363-404). */
+FASTFFT_API fastfft_status fastfft_fwd_input_dims(fastfft_handle h, int dims[4]);
+FASTFFT_API fastfft_status fastfft_fwd_output_dims(fastfft_handle h, int dims[4]);
+FASTFFT_API fastfft_status fastfft_inv_input_dims(fastfft_handle h, int dims[4]);
+FASTFFT_API fastfft_status fastfft_inv_output_dims(fastfft_handle h, int dims[4]);
+/* Bytes of the internal work buffer (the reference's buffer_1/buffer_2 pair). */
+FASTFFT_API fastfft_status fastfft_buffer_bytes(fastfft_handle h, long long* n);
+
+/* Wait() (FastFFT.h:124-126): synchronise the handle's stream. */
+FASTFFT_API fastfft_status fastfft_wait(fastfft_handle h);
+
+/* Message of the last failed call on h ("" if none); static text for a NULL handle. */
+FASTFFT_API const char* fastfft_last_error(fastfft_handle h);
+FASTFFT_API const char* fastfft_status_string(int status);
+/* Library version string. */
+FASTFFT_API const char* fastfft_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTFFT_B200_CAPI_H */

@@ -1,0 +1,116 @@
+"""C ABI checks that need no GPU: exported symbols, plan validation, size queries.
+
+The size queries must return the reference's numbers (ReturnPaddedMemorySize,
+include/FastFFT.h:363-404) and the validation must reject what ValidateDimensions
+rejects (src/fastfft/FastFFT.cu:803-930), with a status code instead of abort().
+"""
+import ctypes
+import os
+import re
+
+import pytest
+
+import fastfft_b200 as F
+from fastfft_b200 import _capi as C
+from oracle import fastfft_oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "fastfft_capi.h")).read()
+    return sorted(set(re.findall(r"FASTFFT_API\s+[\w\s\*]+?\b(fastfft_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(str(C.LIB_PATH))
+    names = header_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(C.SIGNATURES), "binding and header disagree"
+
+
+def test_version_and_status_strings():
+    lib = C.lib()
+    assert b"sm_100a" in lib.fastfft_version()
+    assert lib.fastfft_status_string(C.ERR_INVALID_DIMS) == b"invalid dimensions"
+
+
+def new(rank=2, input_dtype="float32"):
+    return F.FourierTransformer(input_dtype=input_dtype, rank=rank)
+
+
+@pytest.mark.parametrize("fin,fout,iout", [
+    ((64, 64, 1), (512, 512, 1), (512, 512, 1)),
+    ((384, 384, 1), (4096, 4096, 1), (1024, 1024, 1)),
+    ((385, 200, 1), (4096, 2048, 1), (1000, 999, 1)),
+    ((4096, 4096, 1), (4096, 4096, 1), (4096, 4096, 1)),
+    ((64, 64, 64), (256, 256, 256), (128, 128, 128)),
+])
+def test_memory_sizes_match_reference(fin, fout, iout):
+    ft = new(rank=3 if fout[2] > 1 else 2)
+    ft.SetForwardFFTPlan(*fin, *fout)
+    ft.SetInverseFFTPlan(*fout, *iout)
+    assert ft.ReturnInputMemorySize() == O.padded_memory_size(fin)
+    assert ft.ReturnFwdOutputMemorySize() == O.padded_memory_size(fout)
+    assert ft.ReturnInvOutputMemorySize() == O.padded_memory_size(iout)
+    assert ft.ReturnFwdInputDimensions() == (*fin, O.padded_x(fin[0])[0])
+    assert ft.ReturnFwdOutputDimensions() == (*fout, O.padded_x(fout[0])[0])
+    assert ft.ReturnInvOutputDimensions() == (*iout, O.padded_x(iout[0])[0])
+
+
+@pytest.mark.parametrize("fin,fout,iin,iout,status", [
+    ((64, 64, 1), (512, 512, 1), (256, 256, 1), (256, 256, 1), C.ERR_INVALID_DIMS),  # fwd out != inv in
+    ((64, 128, 1), (128, 64, 1), (128, 64, 1), (128, 64, 1), C.ERR_INVALID_DIMS),    # mixed grow/shrink
+    ((100, 100, 1), (100, 100, 1), (100, 100, 1), (100, 100, 1), C.ERR_INVALID_DIMS),  # non-pow2, no pad
+    ((64, 64, 1), (384, 384, 1), (384, 384, 1), (384, 384, 1), C.ERR_INVALID_DIMS),  # non-pow2 fwd out
+    ((64, 64, 1), (512, 512, 1), (512, 512, 1), (600, 600, 1), C.ERR_INVALID_DIMS),  # inverse grows, non-pow2
+    ((64, 64, 64), (1024, 1024, 1024), (1024, 1024, 1024), (1024, 1024, 1024), C.ERR_INVALID_DIMS),  # 3D > 512
+    ((64, 64, 1), (16384, 16384, 1), (16384, 16384, 1), (16384, 16384, 1), C.ERR_UNSUPPORTED),  # > 8192
+    ((4, 4, 1), (8, 8, 1), (8, 8, 1), (8, 8, 1), C.ERR_UNSUPPORTED),  # < 16
+])
+def test_validation_rejects(fin, fout, iin, iout, status):
+    ft = new(rank=3 if fout[2] > 1 else 2)
+    ft.SetForwardFFTPlan(*fin, *fout)
+    with pytest.raises(F.FastFFTError) as e:
+        ft.SetInverseFFTPlan(*iin, *iout)
+    assert e.value.status == status
+
+
+def test_rank_mismatch_rejected():
+    ft = new(rank=3)
+    ft.SetForwardFFTPlan(64, 64, 1, 128, 128, 1)
+    with pytest.raises(F.FastFFTError) as e:
+        ft.SetInverseFFTPlan(128, 128, 1, 128, 128, 1)
+    assert e.value.status == C.ERR_INVALID_DIMS
+
+
+def test_transform_before_plan_is_an_error():
+    ft = new()
+    with pytest.raises(F.FastFFTError) as e:
+        ft.FwdFFT(0x1000)
+    assert e.value.status in (C.ERR_INVALID_ARGUMENT, C.ERR_NOT_PLANNED)
+
+
+def test_bad_dtypes_and_zero_dims():
+    with pytest.raises(F.FastFFTError):
+        C.lib()  # loads
+        h = C.Handle()
+        st = C.lib().fastfft_create(ctypes.byref(h), 0, C.DTYPE_C64, C.DTYPE_C64, 2)
+        raise F.FastFFTError(st, "real input required") if st != C.OK else AssertionError("accepted complex input")
+    ft = new()
+    with pytest.raises(F.FastFFTError) as e:
+        ft.SetForwardFFTPlan(0, 64, 1, 64, 64, 1)
+    assert e.value.status == C.ERR_INVALID_DIMS
+    with pytest.raises(F.FastFFTError) as e:
+        ft.SetForwardFFTPlan(64, 64, 1, 64, 64, 1, is_padded_output=False)
+    assert e.value.status == C.ERR_UNSUPPORTED
+
+
+def test_null_handle_calls_fail_cleanly():
+    lib = C.lib()
+    assert lib.fastfft_set_stream(None, None) == C.ERR_INVALID_ARGUMENT
+    assert lib.fastfft_wait(None) == C.ERR_INVALID_ARGUMENT
+    assert lib.fastfft_destroy(None) == C.OK
+    assert lib.fastfft_last_error(None) != b""
