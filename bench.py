@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Batched 2D padded cross-correlation benchmark (templates/s at 4096^2).
+
+Workload: a 4096x4096 search image (N(0,1) noise + 20 Gaussian blobs, sigma 8, amplitude
+5; seeded, synthetic) whose FP32 spectrum is resident in HBM; 384x384 N(0,1) templates,
+each zero-padded to 4096^2, forward transformed, multiplied by conj(template) x image
+spectrum, inverse transformed and cropped to the 1024x1024 window at the origin
+(FourierTransformer::FwdImageInvFFT with a forward increase and an inverse decrease).
+
+One step = TEMPLATES_PER_STEP templates per GPU through fastfft_fwd_image_inv_many.
+Three different image spectra (3 x 67 MB > 126 MB L2) rotate template by template, so
+every template streams its image spectrum from HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs the same work on its own GPU (templates shard across
+GPUs, no collective in the data path; weak scaling); the elapsed device time is the max
+over ranks.  --impl reference times the host CPU implementation of the same transform
+(the FP32 restatement in oracle/, multithreaded pocketfft) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "xcorr templates/s @4096² (TC split-prec vs FP32, ≤1e-4 rel), % HBM roofline"
+UNIT = "templates/s"
+N, L, W = 4096, 384, 1024
+TEMPLATES_PER_STEP = 64
+N_IMAGES = 3
+# compulsory HBM bytes per template: template read + full image spectrum read + window write
+ALG_BYTES_PER_TEMPLATE = L * L * 4 + (N // 2 + 1) * N * 8 + W * W * 4
+FALLBACK_HBM_GBS = 6650.0
+
+
+def config(templates_per_step):
+    return {
+        "workload": "2D fused cross-correlation FP32: 384^2 template zero-padded to 4096^2, conj-multiply with a "
+                    "resident 4096^2 image spectrum, inverse cropped to a 1024^2 window",
+        "transform": [N, N], "template": [L, L], "window": [W, W],
+        "templates_per_step": templates_per_step,
+        "image_spectra": N_IMAGES,
+        "l2": "3 rotating 67 MB image spectra per GPU (201 MB > 126 MB L2): every template streams its image "
+              "spectrum from HBM",
+        "parallelism": "templates sharded across GPUs, image spectrum replicated (no collective)",
+    }
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic_per_template():
+    """DRAM bytes (read + write) per launch of the fused column kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "xcorr_cols_4096_template384_window1024.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 6:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=5)
+        self.thread.join(timeout=5)
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[2 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+
+        backend = "nccl" if os.environ.get("FASTFFT_BENCH_BACKEND", "nccl") == "nccl" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world, torch):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, value, torch, device):
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU implementation of the same transform (reference arm and cpu_baseline)
+# ---------------------------------------------------------------------------
+def cpu_xcorr_runner(cores):
+    from oracle import fastfft_oracle as O
+
+    from fastfft_b200.workloads import blob_image, to_padded
+
+    img = blob_image(N)
+    spec = O.fwd(to_padded(img), (N, N, 1), (N, N, 1), dtype=np.float32, workers=cores).astype(np.complex64)
+    plan = O.Plan((L, L, 1), (N, N, 1), (N, N, 1), (W, W, 1))
+    rng = np.random.default_rng(O.SEED_BASE + 1)
+
+    def one():
+        t = to_padded(rng.standard_normal((L, L)).astype(np.float32))
+        return O.fwd_image_inv(t, spec, plan, dtype=np.float32, workers=cores)
+
+    return one
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import fastfft_oracle as O
+
+    cores = O.cpu_workers()
+    one = cpu_xcorr_runner(cores)
+    for _ in range(args.warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    sample = f"{args.steps} templates, one per step (384^2 -> 4096^2 -> 1024^2, FP32 pocketfft)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config(1),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+
+    import fastfft_b200 as F
+    from fastfft_b200.workloads import blob_image, to_padded
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    B = args.templates_per_step
+
+    # resident image spectra, prepared on the GPU by the library's own 4096^2 R2C
+    prep = F.FourierTransformer()
+    prep.SetForwardFFTPlan(N, N, 1, N, N, 1)
+    prep.SetInverseFFTPlan(N, N, 1, N, N, 1)
+    images = []
+    for i in range(N_IMAGES):
+        x = torch.from_numpy(to_padded(blob_image(N, seed=20261203 + 2 + 100 * i))).to(dev)
+        spec = torch.empty(prep.ReturnFwdOutputMemorySize(), dtype=torch.float32, device=dev)
+        prep.FwdFFT(x, spec)
+        images.append(spec)
+        del x
+    del prep
+
+    ft = F.FourierTransformer()
+    ft.SetForwardFFTPlan(L, L, 1, N, N, 1)
+    ft.SetInverseFFTPlan(N, N, 1, W, W, 1)
+    n_in, n_out = ft.ReturnInputMemorySize(), ft.ReturnInvOutputMemorySize()
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(20261203 + 1 + 1000 * rank)
+    templates = torch.zeros(B, n_in, dtype=torch.float32, device=dev)
+    templates.view(B, L, -1)[:, :, :L] = torch.randn(B, L, L, device=dev, generator=gen)
+    outputs = torch.empty(B, n_out, dtype=torch.float32, device=dev)
+    ins = [templates[i] for i in range(B)]
+    outs = [outputs[i] for i in range(B)]
+    imgs = [images[i % N_IMAGES] for i in range(B)]
+
+    def step():
+        ft.FwdImageInvFFTMany(ins, imgs, outs)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region (device-resident inputs) ----
+    clocks = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    launches0 = ft.LaunchCount()
+    ft.ProfileStart(args.steps * B)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world, torch)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world, torch)
+    pass_ms, n_calls = ft.ProfileStop()
+    launches = ft.LaunchCount() - launches0
+    ms = max_over_ranks(world, e0.elapsed_time(e1), torch, dev)
+    value = world * args.steps * B / (ms * 1e-3)
+
+    # dominant kernel: the fused column pass (pass 1); the others reported beside it
+    per_pass_us = [1e3 * p / max(n_calls, 1) for p in pass_ms]
+    dom = int(np.argmax(per_pass_us))
+    peak, peak_kind = measured_hbm_peak()
+    achieved = ALG_BYTES_PER_TEMPLATE / (per_pass_us[dom] * 1e-6) / 1e9
+    traffic = ncu_traffic_per_template()
+
+    # ---- end to end: pinned host templates in, windows back to pinned host ----
+    h_in = torch.empty(B, n_in, dtype=torch.float32, pin_memory=True)
+    h_in.copy_(templates.cpu())
+    h_out = torch.empty(B, n_out, dtype=torch.float32, pin_memory=True)
+    e2e_steps = max(1, min(args.steps, 10))
+    for _ in range(1):
+        templates.copy_(h_in, non_blocking=True)
+        step()
+        h_out.copy_(outputs, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world, torch)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(e2e_steps):
+        templates.copy_(h_in, non_blocking=True)
+        step()
+        h_out.copy_(outputs, non_blocking=True)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(world, f0.elapsed_time(f1), torch, dev)
+    e2e_value = world * e2e_steps * B / (e2e_ms * 1e-3)
+
+    # ---- cuFFT pad-then-transform comparator (torch.fft) ----
+    cufft = None
+    if rank == 0 and not args.skip_cufft:
+        spec_c = images[0].view(torch.complex64).view(N // 2 + 1, N).t()  # [ky][kx]
+
+        def cufft_one(i):
+            p = torch.zeros(N, N, device=dev)
+            p[:L, :L] = templates[i].view(L, -1)[:, :L]
+            s = torch.fft.rfft2(p)
+            r = torch.fft.irfft2(torch.conj(s) * spec_c, s=(N, N))
+            return r[:W, :W].contiguous()
+
+        for i in range(3):
+            cufft_one(i)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 20
+        g0.record()
+        for i in range(reps):
+            cufft_one(i % B)
+        g1.record()
+        torch.cuda.synchronize()
+        cufft_v = reps / (g0.elapsed_time(g1) * 1e-3)
+        cufft = {"value": cufft_v, "unit": UNIT, "how": "torch.fft (cuFFT): pad, rfft2, conj-multiply, irfft2, crop",
+                 "ours_over_cufft": value / world / cufft_v}
+
+    # ---- CPU baseline (rank 0, one GPU) and accuracy check of one window ----
+    cpu = None
+    accuracy = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        from oracle import fastfft_oracle as O
+
+        cores = O.cpu_workers()
+        one = cpu_xcorr_runner(cores)
+        one()
+        t0 = time.perf_counter()
+        n_cpu = 0
+        while n_cpu < 3 or time.perf_counter() - t0 < args.cpu_seconds:
+            one()
+            n_cpu += 1
+        dt = time.perf_counter() - t0
+        cpu = {"value": n_cpu / dt, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{n_cpu} templates (384^2 -> 4096^2 -> 1024^2, FP32 pocketfft, {cores} threads)"}
+        # accuracy of template 0 against the FP64 oracle
+        spec0 = images[0].cpu().numpy().view(np.complex64).reshape(1, N // 2 + 1, N)
+        plan = O.Plan((L, L, 1), (N, N, 1), (N, N, 1), (W, W, 1))
+        ref = O.real_from_padded(O.fwd_image_inv(templates[0].cpu().numpy(), spec0, plan, out_dtype=np.float64),
+                                 (W, W, 1))
+        got = O.real_from_padded(outputs[0].cpu().numpy(), (W, W, 1))
+        gi, _, _ = O.peak(got)
+        ri, rtop, margin = O.peak(ref)
+        accuracy = {"rel_l2_vs_fp64": O.rel_l2(got, ref), "rel_max_vs_fp64": O.rel_max(got, ref),
+                    "peak_index_exact": bool(gi == ri), "peak_margin_rel": margin / abs(rtop)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config(B),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": ["r2c_rows", "cols_xcorr", "c2r_rows"][dom],
+                         "algorithmic_bytes_per_launch": ALG_BYTES_PER_TEMPLATE,
+                         "pass_us_per_template": per_pass_us,
+                         "pipeline_frac": ALG_BYTES_PER_TEMPLATE / (ms * 1e-3 / (args.steps * B)) / 1e9 / peak},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": B * n_in * 4,
+                    "d2h_bytes_per_step": B * n_out * 4, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cufft_pad_then_transform": cufft,
+            "accuracy": accuracy,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--templates-per-step", type=int, default=TEMPLATES_PER_STEP)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-cufft", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

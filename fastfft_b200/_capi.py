@@ -59,6 +59,11 @@ SIGNATURES = {
     "fastfft_fwd": (_st, [Handle, _vp, _vp, _op, _op]),
     "fastfft_inv": (_st, [Handle, _vp, _vp, _op, _op]),
     "fastfft_fwd_image_inv": (_st, [Handle, _vp, _vp, _vp, _op, _op, _op]),
+    "fastfft_fwd_image_inv_many": (_st, [Handle, ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                         ctypes.POINTER(_vp), _op, _op, _op]),
+    "fastfft_launch_count": (_st, [Handle, _ll]),
+    "fastfft_profile_start": (_st, [Handle, ctypes.c_int]),
+    "fastfft_profile_stop": (_st, [Handle, ctypes.POINTER(ctypes.c_double), ctypes.c_int, _ll]),
     "fastfft_input_memory_size": (_st, [Handle, _ll]),
     "fastfft_fwd_output_memory_size": (_st, [Handle, _ll]),
     "fastfft_inv_output_memory_size": (_st, [Handle, _ll]),

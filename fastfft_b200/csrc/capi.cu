@@ -164,6 +164,27 @@ fastfft_status prepare_call(fastfft_plan_s* h) {
 float2* region_a(fastfft_plan_s* h) { return static_cast<float2*>(h->buffer); }
 float2* region_b(fastfft_plan_s* h) { return reinterpret_cast<float2*>(static_cast<char*>(h->buffer) + h->bytes_a); }
 
+// Per-pass timing marks (no-ops unless profiling is on).
+void prof_begin_call(fastfft_plan_s* h) {
+    if (!h->prof_events || h->prof_calls >= h->prof_capacity) return;
+    h->prof_mark = 0;
+    cudaEventRecord(h->prof_events[h->prof_calls * fastfft_plan_s::kProfMarks], h->stream);
+    h->prof_mark = 1;
+}
+void prof_mark(fastfft_plan_s* h) {
+    if (!h->prof_events || h->prof_calls >= h->prof_capacity) return;
+    if (h->prof_mark <= 0 || h->prof_mark >= fastfft_plan_s::kProfMarks) return;
+    cudaEventRecord(h->prof_events[h->prof_calls * fastfft_plan_s::kProfMarks + h->prof_mark], h->stream);
+    h->prof_mark++;
+}
+void prof_end_call(fastfft_plan_s* h) {
+    if (!h->prof_events || h->prof_calls >= h->prof_capacity) return;
+    // unused marks of a shorter call repeat the last one (zero-length passes)
+    while (h->prof_mark > 0 && h->prof_mark < fastfft_plan_s::kProfMarks) prof_mark(h);
+    h->prof_calls++;
+    h->prof_mark = 0;
+}
+
 // Row pass of the forward transform into region A.
 fastfft_status run_fwd_rows(fastfft_plan_s* h, const void* in, float pre_scale, int kmax) {
     const int nx = (int)std::max(h->fwd_in.x, h->fwd_out.x);
@@ -182,6 +203,8 @@ fastfft_status run_fwd_rows(fastfft_plan_s* h, const void* in, float pre_scale, 
     a.tw = tw;
     e = launch_r2c_rows(nx, h->input_dtype, a, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "r2c row pass");
+    h->launches++;
+    prof_mark(h);
     return FASTFFT_OK;
 }
 
@@ -201,6 +224,8 @@ fastfft_status run_inv_rows(fastfft_plan_s* h, void* out, float post_scale) {
     a.tw = tw;
     e = launch_c2r_rows(nx, h->output_dtype, a, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "c2r row pass");
+    h->launches++;
+    prof_mark(h);
     return FASTFFT_OK;
 }
 
@@ -235,6 +260,10 @@ fastfft_status fastfft_destroy(fastfft_handle h) {
     if (h->buffer) {
         cudaStreamSynchronize(h->stream);
         cudaFree(h->buffer);
+    }
+    if (h->prof_events) {
+        for (int i = 0; i < h->prof_capacity * fastfft_plan_s::kProfMarks; i++) cudaEventDestroy(h->prof_events[i]);
+        delete[] h->prof_events;
     }
     delete h;
     return FASTFFT_OK;
@@ -316,6 +345,7 @@ fastfft_status fastfft_fwd(fastfft_handle h, const void* input, void* output, co
     if (st != FASTFFT_OK) return st;
     void* out = output ? output : const_cast<void*>(input);
     const int kmax = (int)h->fwd_out.w;
+    prof_begin_call(h);
     st = run_fwd_rows(h, input, scale_of(pre_op), kmax);
     if (st != FASTFFT_OK) return st;
     const int ny = (int)std::max(h->fwd_in.y, h->fwd_out.y);
@@ -337,6 +367,9 @@ fastfft_status fastfft_fwd(fastfft_handle h, const void* input, void* output, co
     c.tw = tw;
     e = launch_cols_fwd(ny, c, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "forward column pass");
+    h->launches++;
+    prof_mark(h);
+    prof_end_call(h);
     return FASTFFT_OK;
 }
 
@@ -353,6 +386,7 @@ fastfft_status fastfft_inv(fastfft_handle h, const void* input, void* output, co
         return fail(h, FASTFFT_ERR_UNSUPPORTED, "inverse size increase is not supported");
     void* out = output ? output : const_cast<void*>(input);
     const int ny = (int)h->inv_in.y;
+    prof_begin_call(h);
     const float2* tw = nullptr;
     cudaError_t e = twiddles_for(ny, &tw);
     if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
@@ -371,14 +405,15 @@ fastfft_status fastfft_inv(fastfft_handle h, const void* input, void* output, co
     c.tw = tw;
     e = launch_cols_inv(ny, c, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "inverse column pass");
-    return run_inv_rows(h, out, scale_of(post_op));
+    h->launches++;
+    prof_mark(h);
+    st = run_inv_rows(h, out, scale_of(post_op));
+    prof_end_call(h);
+    return st;
 }
 
-fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const void* image_spectrum, void* output,
-                                     const fastfft_op* pre_op, const fastfft_op* intra_op,
-                                     const fastfft_op* post_op) {
-    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
-    if (!input || !image_spectrum) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image pointer");
+static fastfft_status xcorr_checks(fastfft_handle h, const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                   const fastfft_op* post_op) {
     if (!valid_op(pre_op, false)) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "pre-op must be NOOP or SCALE");
     if (!valid_op(post_op, false)) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "post-op must be NOOP or SCALE");
     if (!valid_op(intra_op, true))
@@ -389,9 +424,14 @@ fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const 
         return fail(h, FASTFFT_ERR_UNSUPPORTED, "cross-correlation with a forward size decrease is not supported");
     if (h->inv_change == SizeChange::Increase)
         return fail(h, FASTFFT_ERR_UNSUPPORTED, "cross-correlation with an inverse size increase is not supported");
-    void* out = output ? output : const_cast<void*>(input);
+    return FASTFFT_OK;
+}
+
+static fastfft_status xcorr_one(fastfft_handle h, const void* input, const void* image_spectrum, void* out,
+                                const fastfft_op* pre_op, const fastfft_op* intra_op, const fastfft_op* post_op) {
     const int nx = (int)h->fwd_out.x;
-    st = run_fwd_rows(h, input, scale_of(pre_op), nx / 2 + 1);
+    prof_begin_call(h);
+    fastfft_status st = run_fwd_rows(h, input, scale_of(pre_op), nx / 2 + 1);
     if (st != FASTFFT_OK) return st;
     const int ny = (int)h->fwd_out.y;
     const float2* tw = nullptr;
@@ -415,7 +455,98 @@ fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const 
     c.tw = tw;
     e = launch_cols_xcorr(ny, h->image_dtype, c, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "cross-correlation column pass");
-    return run_inv_rows(h, out, scale_of(post_op));
+    h->launches++;
+    prof_mark(h);
+    st = run_inv_rows(h, out, scale_of(post_op));
+    prof_end_call(h);
+    return st;
+}
+
+fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const void* image_spectrum, void* output,
+                                     const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                     const fastfft_op* post_op) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (!input || !image_spectrum) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image pointer");
+    fastfft_status st = xcorr_checks(h, pre_op, intra_op, post_op);
+    if (st != FASTFFT_OK) return st;
+    return xcorr_one(h, input, image_spectrum, output ? output : const_cast<void*>(input), pre_op, intra_op, post_op);
+}
+
+fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, const void* const* inputs,
+                                          const void* const* image_spectra, void* const* outputs,
+                                          const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                          const fastfft_op* post_op) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (n < 0 || (n > 0 && (!inputs || !image_spectra)))
+        return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image array");
+    for (int i = 0; i < n; i++)
+        if (!inputs[i] || !image_spectra[i])
+            return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image pointer in the batch");
+    fastfft_status st = xcorr_checks(h, pre_op, intra_op, post_op);
+    if (st != FASTFFT_OK) return st;
+    for (int i = 0; i < n; i++) {
+        void* out = (outputs && outputs[i]) ? outputs[i] : const_cast<void*>(inputs[i]);
+        st = xcorr_one(h, inputs[i], image_spectra[i], out, pre_op, intra_op, post_op);
+        if (st != FASTFFT_OK) return st;
+    }
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_launch_count(fastfft_handle h, long long* n) {
+    if (!h || !n) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null argument");
+    *n = h->launches;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_profile_start(fastfft_handle h, int max_calls) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (max_calls <= 0) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "max_calls must be > 0");
+    if (h->prof_events) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "profiling is already on");
+    const int n = max_calls * fastfft_plan_s::kProfMarks;
+    cudaEvent_t* ev = new (std::nothrow) cudaEvent_t[n];
+    if (!ev) return fail(h, FASTFFT_ERR_ALLOC, "out of host memory");
+    for (int i = 0; i < n; i++) {
+        cudaError_t e = cudaEventCreate(&ev[i]);
+        if (e != cudaSuccess) {
+            for (int k = 0; k < i; k++) cudaEventDestroy(ev[k]);
+            delete[] ev;
+            return cuda_fail(h, e, "cudaEventCreate");
+        }
+    }
+    h->prof_events = ev;
+    h->prof_capacity = max_calls;
+    h->prof_calls = 0;
+    h->prof_mark = 0;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_profile_stop(fastfft_handle h, double* pass_ms, int n_pass, long long* n_calls) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (!h->prof_events) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "profiling is not on");
+    constexpr int M = fastfft_plan_s::kProfMarks;
+    fastfft_status st = FASTFFT_OK;
+    double acc[M - 1] = {0, 0, 0};
+    for (int c = 0; c < h->prof_calls && st == FASTFFT_OK; c++) {
+        for (int p = 0; p < M - 1; p++) {
+            cudaError_t e = cudaEventSynchronize(h->prof_events[c * M + p + 1]);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, h->prof_events[c * M + p], h->prof_events[c * M + p + 1]);
+            if (e != cudaSuccess) {
+                st = cuda_fail(h, e, "profile events");
+                break;
+            }
+            acc[p] += ms;
+        }
+    }
+    if (pass_ms)
+        for (int p = 0; p < n_pass && p < M - 1; p++) pass_ms[p] = acc[p];
+    if (n_calls) *n_calls = h->prof_calls;
+    for (int i = 0; i < h->prof_capacity * M; i++) cudaEventDestroy(h->prof_events[i]);
+    delete[] h->prof_events;
+    h->prof_events = nullptr;
+    h->prof_capacity = 0;
+    h->prof_calls = 0;
+    return st;
 }
 
 static fastfft_status get_ll(fastfft_handle h, long long* n, long long v) {

@@ -43,4 +43,15 @@ struct fastfft_plan_s {
 
     cudaStream_t stream = cudaStreamPerThread;
     std::string last_error;
+
+    // kernels launched through this handle (fastfft_launch_count)
+    long long launches = 0;
+
+    // optional per-pass timing: events recorded before the first pass and after each
+    // pass of every transform call while profiling is on (fastfft_profile_start/stop)
+    static constexpr int kProfMarks = 4;
+    cudaEvent_t* prof_events = nullptr;
+    int prof_capacity = 0;  // calls
+    int prof_calls = 0;
+    int prof_mark = 0;      // next mark within the current call
 };

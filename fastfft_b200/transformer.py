@@ -78,8 +78,12 @@ class FourierTransformer:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            self._lib.fastfft_destroy(h)
+        lib = getattr(self, "_lib", None)
+        if h is not None and h.value and lib is not None:
+            try:
+                lib.fastfft_destroy(h)
+            except Exception:  # interpreter shutdown: the library may already be gone
+                pass
             self._h = C.Handle()
 
     # -- helpers ---------------------------------------------------------
@@ -128,6 +132,41 @@ class FourierTransformer:
         self._bind_stream()
         self._check(self._lib.fastfft_fwd_image_inv(self._h, _ptr(input_ptr), _ptr(image_to_search), _ptr(output_ptr),
                                                     _opref(pre_op), _opref(intra_op), _opref(post_op)))
+
+    def FwdImageInvFFTMany(self, inputs, images, outputs=None, pre_op=None, intra_op=None, post_op=None):
+        """FwdImageInvFFT over a list of templates in one library call.
+
+        images is one image (searched by every template) or a list with one image per
+        template; outputs is a list of the same length as inputs, or None (in place).
+        """
+        n = len(inputs)
+        if not isinstance(images, (list, tuple)):
+            images = [images] * n
+        if len(images) != n or (outputs is not None and len(outputs) != n):
+            raise ValueError("inputs, images and outputs must have the same length")
+        if intra_op is None:
+            intra_op = KernelFunction.conj_mul()
+        arr = ctypes.c_void_p * n
+        ins = arr(*[_ptr(x) for x in inputs])
+        ims = arr(*[_ptr(x) for x in images])
+        outs = arr(*[_ptr(x) for x in outputs]) if outputs is not None else None
+        self._bind_stream()
+        self._check(self._lib.fastfft_fwd_image_inv_many(self._h, n, ins, ims, outs, _opref(pre_op), _opref(intra_op),
+                                                         _opref(post_op)))
+
+    # -- accounting and profiling ------------------------------------------
+    def LaunchCount(self):
+        return self._ll(self._lib.fastfft_launch_count)
+
+    def ProfileStart(self, max_calls):
+        self._check(self._lib.fastfft_profile_start(self._h, int(max_calls)))
+
+    def ProfileStop(self):
+        """Returns ([ms of pass 0, 1, 2 summed over the recorded calls], n_calls)."""
+        ms = (ctypes.c_double * 3)()
+        n = ctypes.c_longlong()
+        self._check(self._lib.fastfft_profile_stop(self._h, ms, 3, ctypes.byref(n)))
+        return list(ms), n.value
 
     def Wait(self):
         self._check(self._lib.fastfft_wait(self._h))

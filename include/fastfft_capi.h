@@ -105,6 +105,16 @@ FASTFFT_API fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* i
                                      const fastfft_op* pre_op, const fastfft_op* intra_op,
                                      const fastfft_op* post_op);
 
+/* Many templates in one call: FwdImageInvFFT of inputs[i] against image_spectra[i] into
+ * outputs[i] (NULL entries or a NULL array mean in place), i < n, all on the handle's
+ * stream (pass the same image pointer n times to search one image).  The reference
+ * correlates one template per FwdImageInvFFT call (FastFFT.cu:295-313); this is that
+ * call repeated without a host round trip per template. */
+FASTFFT_API fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, const void* const* inputs,
+                                                      const void* const* image_spectra, void* const* outputs,
+                                                      const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                                      const fastfft_op* post_op);
+
 /* ReturnInputMemorySize / ReturnFwdOutputMemorySize / ReturnInvOutputMemorySize
  * (FastFFT.h:194-204): element counts of InputType, FFTW-padded. */
 FASTFFT_API fastfft_status fastfft_input_memory_size(fastfft_handle h, long long* n);
@@ -118,6 +128,15 @@ FASTFFT_API fastfft_status fastfft_inv_input_dims(fastfft_handle h, int dims[4])
 FASTFFT_API fastfft_status fastfft_inv_output_dims(fastfft_handle h, int dims[4]);
 /* Bytes of the internal work buffer (the reference's buffer_1/buffer_2 pair). */
 FASTFFT_API fastfft_status fastfft_buffer_bytes(fastfft_handle h, long long* n);
+
+/* Number of kernels this handle has launched (for launch accounting in benchmarks). */
+FASTFFT_API fastfft_status fastfft_launch_count(fastfft_handle h, long long* n);
+/* Per-pass device timing with CUDA events on the work stream, for up to max_calls
+ * transform calls.  stop() waits for the events and returns the summed milliseconds of
+ * pass 0/1/2 (row pass, column pass, row pass) over the recorded calls.  The reference
+ * times with CUDA events in its test harness only (src/fastfft/Image.cuh:64-84). */
+FASTFFT_API fastfft_status fastfft_profile_start(fastfft_handle h, int max_calls);
+FASTFFT_API fastfft_status fastfft_profile_stop(fastfft_handle h, double* pass_ms, int n_pass, long long* n_calls);
 
 /* Wait() (FastFFT.h:124-126): synchronise the handle's stream. */
 FASTFFT_API fastfft_status fastfft_wait(fastfft_handle h);

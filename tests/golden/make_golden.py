@@ -48,7 +48,7 @@ def main():
     L, N = 32, 128
     a = rng.standard_normal((L, L)).astype(np.float32).astype(np.float64)
     s = fwd_full(a, N)
-    spec = s[:, : N // 2 + 1].T[None]            # [kz][kx][ky]
+    spec = np.ascontiguousarray(s[:, : N // 2 + 1].T[None])  # [kz][kx][ky]
     rt = inv_full(s[:, : N // 2 + 1], N)
     np.savez_compressed(os.path.join(HERE, "fwd_32_to_128.npz"), fwd_in=(L, L, 1), fwd_out=(N, N, 1),
                         inv_in=(N, N, 1), inv_out=(N, N, 1), input=pad_rows(a, L), spectrum=spec,
@@ -62,7 +62,7 @@ def main():
     c = inv_full(np.conj(st) * si, N)[:W, :W]
     np.savez_compressed(os.path.join(HERE, "xcorr_48_to_128_w40.npz"), fwd_in=(L, L, 1), fwd_out=(N, N, 1),
                         inv_in=(N, N, 1), inv_out=(W, W, 1), input=pad_rows(t, L),
-                        image_spectrum=si.T[None].astype(np.complex128), output=pad_rows(c, W))
+                        image_spectrum=np.ascontiguousarray(si.T[None]).astype(np.complex128), output=pad_rows(c, W))
 
 
 if __name__ == "__main__":
