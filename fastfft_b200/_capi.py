@@ -62,6 +62,8 @@ SIGNATURES = {
     "fastfft_fwd_image_inv_many": (_st, [Handle, ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                                          ctypes.POINTER(_vp), _op, _op, _op]),
     "fastfft_launch_count": (_st, [Handle, _ll]),
+    "fastfft_set_full_size_correlation": (_st, [Handle, ctypes.c_int]),
+    "fastfft_correlation_size": (_st, [Handle, _dims]),
     "fastfft_profile_start": (_st, [Handle, ctypes.c_int]),
     "fastfft_profile_stop": (_st, [Handle, ctypes.POINTER(ctypes.c_double), ctypes.c_int, _ll]),
     "fastfft_input_memory_size": (_st, [Handle, _ll]),

@@ -11,6 +11,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/fastfft_capi.h"
 #include "kernels_2d.cuh"
@@ -110,6 +111,12 @@ fastfft_status validate(fastfft_plan_s* h) {
 // Internal buffer layout (the reference's buffer_1 / buffer_2 pair):
 //   region A: [kx][y] forward row-pass output, pitch pA >= L_y (multiple of 4)
 //   region B: [kx][y] inverse column-pass output, pitch pB >= W_y (multiple of 4)
+long long pow2_at_least(long long v) {
+    long long p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
 void size_buffers(fastfft_plan_s* h) {
     const long long nx_f = std::max(h->fwd_in.x, h->fwd_out.x);
     h->pitch_a = round_up(h->fwd_in.y, 4);
@@ -118,11 +125,30 @@ void size_buffers(fastfft_plan_s* h) {
     h->pitch_b = round_up(h->inv_out.y, 4);
     const long long kx_i = h->inv_in.x / 2 + 1;
     h->bytes_b = round_up(kx_i * h->pitch_b * 8, 256);
+    // reduced-size correlation
+    h->red_ok = false;
+    h->bytes_c = 0;
+    if (h->rank == 2 && h->fwd_change != SizeChange::Decrease && h->inv_change == SizeChange::Decrease) {
+        const long long nx = h->fwd_out.x, ny = h->fwd_out.y;
+        const long long mx = std::min(nx, std::max<long long>(ffb::kMinN, pow2_at_least(h->fwd_in.x + h->inv_out.x - 1)));
+        const long long my = std::min(ny, std::max<long long>(ffb::kMinN, pow2_at_least(h->fwd_in.y + h->inv_out.y - 1)));
+        if (mx < nx || my < ny) {
+            h->red_ok = true;
+            h->red_mx = mx;
+            h->red_my = my;
+            const long long stage = std::max((nx / 2 + 1) * my, (mx / 2 + 1) * my) * 8;  // [kx][y] columns
+            const long long real = my * (2 * (mx / 2 + 1)) * 4;                          // cropped image rows
+            const long long spec = (mx / 2 + 1) * my * 8;                                // reduced spectrum
+            h->off_c_real = round_up(stage, 256);
+            h->off_c_spec = h->off_c_real + round_up(real, 256);
+            h->bytes_c = h->off_c_spec + round_up(spec, 256);
+        }
+    }
 }
 
 fastfft_status allocate(fastfft_plan_s* h) {
     size_buffers(h);
-    const size_t need = (size_t)(h->bytes_a + h->bytes_b);
+    const size_t need = (size_t)(h->bytes_a + h->bytes_b + h->bytes_c);
     if (h->buffer && h->buffer_bytes >= need) return FASTFFT_OK;
     if (h->buffer) {
         cudaFree(h->buffer);
@@ -163,6 +189,7 @@ fastfft_status prepare_call(fastfft_plan_s* h) {
 
 float2* region_a(fastfft_plan_s* h) { return static_cast<float2*>(h->buffer); }
 float2* region_b(fastfft_plan_s* h) { return reinterpret_cast<float2*>(static_cast<char*>(h->buffer) + h->bytes_a); }
+char* region_c(fastfft_plan_s* h) { return static_cast<char*>(h->buffer) + h->bytes_a + h->bytes_b; }
 
 // Per-pass timing marks (no-ops unless profiling is on).
 void prof_begin_call(fastfft_plan_s* h) {
@@ -403,7 +430,7 @@ fastfft_status fastfft_inv(fastfft_handle h, const void* input, void* output, co
     c.out_scale = 1.f;
     c.intra_scale = 1.f;
     c.tw = tw;
-    e = launch_cols_inv(ny, c, h->stream);
+    e = launch_cols_inv(ny, FASTFFT_DTYPE_C64, c, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "inverse column pass");
     h->launches++;
     prof_mark(h);
@@ -462,6 +489,90 @@ static fastfft_status xcorr_one(fastfft_handle h, const void* input, const void*
     return st;
 }
 
+// Prepare the reduced spectrum of one image: C2R of the size-N spectrum keeping
+// [0, My) x [0, Mx), R2C at size M, scaled by 1/(Mx*My) so that the size-M correlation
+// carries the same Nx*Ny factor as the size-N one.
+static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spectrum) {
+    const int nx = (int)h->fwd_out.x, ny = (int)h->fwd_out.y;
+    const int mx = (int)h->red_mx, my = (int)h->red_my;
+    char* c = region_c(h);
+    float2* stage = reinterpret_cast<float2*>(c);
+    float* crop = reinterpret_cast<float*>(c + h->off_c_real);
+    float2* spec = reinterpret_cast<float2*>(c + h->off_c_spec);
+    const long long crop_pitch = 2LL * (mx / 2 + 1);
+    const float2* tw = nullptr;
+    cudaError_t e;
+    // 1. inverse along y, keep y < My: stage[kx][y]
+    if ((e = twiddles_for(ny, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    ColArgs c1;
+    std::memset(&c1, 0, sizeof(c1));
+    c1.in = image_spectrum; c1.in_stride = ny; c1.L = ny;
+    c1.out = stage; c1.out_stride = my; c1.W = my; c1.n_cols = nx / 2 + 1;
+    c1.in_scale = 1.f; c1.out_scale = 1.f; c1.intra_scale = 1.f; c1.tw = tw;
+    if ((e = launch_cols_inv(ny, h->image_dtype, c1, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (inverse columns)");
+    // 2. C2R along x, keep x < Mx: crop[y][x]
+    if ((e = twiddles_for(nx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    RowInvArgs r2;
+    r2.in = stage; r2.in_pitch = my; r2.n_rows = my; r2.out = crop; r2.out_pitch = crop_pitch; r2.W = mx;
+    r2.scale = 1.f; r2.tw = tw;
+    if ((e = launch_c2r_rows(nx, FASTFFT_DTYPE_F32, r2, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (C2R rows)");
+    // 3. R2C along x at size Mx: stage[kx][y]
+    if ((e = twiddles_for(mx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    RowFwdArgs r3;
+    r3.in = crop; r3.in_pitch = crop_pitch; r3.n_rows = my; r3.L = mx; r3.out = stage; r3.out_pitch = my;
+    r3.kmax = mx / 2 + 1; r3.scale = 1.f; r3.tw = tw;
+    if ((e = launch_r2c_rows(mx, FASTFFT_DTYPE_F32, r3, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (R2C rows)");
+    // 4. forward along y at size My, scaled: spec[kx][ky]
+    if ((e = twiddles_for(my, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    ColArgs c4;
+    std::memset(&c4, 0, sizeof(c4));
+    c4.in = stage; c4.in_stride = my; c4.L = my;
+    c4.out = spec; c4.out_stride = my; c4.W = my; c4.n_cols = mx / 2 + 1;
+    c4.in_scale = 1.f; c4.out_scale = 1.f / ((float)mx * (float)my); c4.intra_scale = 1.f; c4.tw = tw;
+    if ((e = launch_cols_fwd(my, c4, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (forward columns)");
+    h->launches += 4;
+    return FASTFFT_OK;
+}
+
+// One template through the reduced-size correlation against the prepared spectrum.
+static fastfft_status red_xcorr_one(fastfft_handle h, const void* input, void* out, const fastfft_op* pre_op,
+                                    const fastfft_op* intra_op, const fastfft_op* post_op) {
+    const int mx = (int)h->red_mx, my = (int)h->red_my;
+    const float2* spec = reinterpret_cast<const float2*>(region_c(h) + h->off_c_spec);
+    const float2* tw = nullptr;
+    cudaError_t e;
+    prof_begin_call(h);
+    if ((e = twiddles_for(mx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    RowFwdArgs a;
+    a.in = input; a.in_pitch = 2LL * h->fwd_in.w; a.n_rows = (int)h->fwd_in.y; a.L = (int)h->fwd_in.x;
+    a.out = region_a(h); a.out_pitch = h->pitch_a; a.kmax = mx / 2 + 1; a.scale = scale_of(pre_op); a.tw = tw;
+    if ((e = launch_r2c_rows(mx, h->input_dtype, a, h->stream)) != cudaSuccess) return cuda_fail(h, e, "r2c row pass");
+    h->launches++;
+    prof_mark(h);
+    if ((e = twiddles_for(my, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    ColArgs c;
+    std::memset(&c, 0, sizeof(c));
+    c.in = region_a(h); c.in_stride = h->pitch_a; c.L = (int)h->fwd_in.y;
+    c.img = spec; c.img_stride = my;
+    c.out = region_b(h); c.out_stride = h->pitch_b; c.W = (int)h->inv_out.y; c.n_cols = mx / 2 + 1;
+    c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
+    c.intra_scale = intra_op ? intra_op->scale : 1.f;
+    c.in_scale = 1.f; c.out_scale = 1.f; c.tw = tw;
+    if ((e = launch_cols_xcorr(my, FASTFFT_DTYPE_C64, c, h->stream)) != cudaSuccess)
+        return cuda_fail(h, e, "cross-correlation column pass");
+    h->launches++;
+    prof_mark(h);
+    if ((e = twiddles_for(mx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    RowInvArgs r;
+    r.in = region_b(h); r.in_pitch = h->pitch_b; r.n_rows = (int)h->inv_out.y;
+    r.out = out; r.out_pitch = 2LL * h->inv_out.w; r.W = (int)h->inv_out.x; r.scale = scale_of(post_op); r.tw = tw;
+    if ((e = launch_c2r_rows(mx, h->output_dtype, r, h->stream)) != cudaSuccess) return cuda_fail(h, e, "c2r row pass");
+    h->launches++;
+    prof_mark(h);
+    prof_end_call(h);
+    return FASTFFT_OK;
+}
+
 fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const void* image_spectrum, void* output,
                                      const fastfft_op* pre_op, const fastfft_op* intra_op,
                                      const fastfft_op* post_op) {
@@ -484,11 +595,47 @@ fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, const void* c
             return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image pointer in the batch");
     fastfft_status st = xcorr_checks(h, pre_op, intra_op, post_op);
     if (st != FASTFFT_OK) return st;
-    for (int i = 0; i < n; i++) {
-        void* out = (outputs && outputs[i]) ? outputs[i] : const_cast<void*>(inputs[i]);
-        st = xcorr_one(h, inputs[i], image_spectra[i], out, pre_op, intra_op, post_op);
-        if (st != FASTFFT_OK) return st;
+    if (!h->red_ok || h->force_full_size) {
+        for (int i = 0; i < n; i++) {
+            void* out = (outputs && outputs[i]) ? outputs[i] : const_cast<void*>(inputs[i]);
+            st = xcorr_one(h, inputs[i], image_spectra[i], out, pre_op, intra_op, post_op);
+            if (st != FASTFFT_OK) return st;
+        }
+        return FASTFFT_OK;
     }
+    // Reduced-size path: templates are grouped by image (in order of first use); each
+    // distinct image is prepared once for the whole call.
+    std::vector<char> done(n, 0);
+    for (int i = 0; i < n; i++) {
+        if (done[i]) continue;
+        const void* img = image_spectra[i];
+        st = red_prepare_image(h, img);
+        if (st != FASTFFT_OK) return st;
+        for (int k = i; k < n; k++) {
+            if (done[k] || image_spectra[k] != img) continue;
+            void* out = (outputs && outputs[k]) ? outputs[k] : const_cast<void*>(inputs[k]);
+            st = red_xcorr_one(h, inputs[k], out, pre_op, intra_op, post_op);
+            if (st != FASTFFT_OK) return st;
+            done[k] = 1;
+        }
+    }
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_set_full_size_correlation(fastfft_handle h, int force) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    h->force_full_size = force != 0;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_correlation_size(fastfft_handle h, int dims[2]) {
+    if (!h || !dims) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null argument");
+    fastfft_status st = validate(h);
+    if (st != FASTFFT_OK) return st;
+    size_buffers(h);
+    const bool red = h->red_ok && !h->force_full_size;
+    dims[0] = (int)(red ? h->red_mx : h->fwd_out.x);
+    dims[1] = (int)(red ? h->red_my : h->fwd_out.y);
     return FASTFFT_OK;
 }
 

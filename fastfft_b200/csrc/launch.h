@@ -17,7 +17,7 @@ struct RowInvArgs;
 cudaError_t launch_r2c_rows(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
 cudaError_t launch_c2r_rows(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
 cudaError_t launch_cols_fwd(int n, const ColArgs& a, cudaStream_t st);
-cudaError_t launch_cols_inv(int n, const ColArgs& a, cudaStream_t st);
+cudaError_t launch_cols_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st);
 
 // Device-wide FP64-generated twiddle table (generated once per device).

@@ -3,13 +3,13 @@
 
 namespace ffb {
 
-template <int N, int MODE, class ImgC>
+template <int N, int MODE, class ImgC, class InC = float2>
 static cudaError_t cols_impl(const ColArgs& a, cudaStream_t st) {
     constexpr int FPB = col_fpb<N>();
     constexpr int THREADS = FftShape<N>::T * FPB;
     const size_t smem = (size_t)FPB * FftShape<N>::SMEM * sizeof(float2);
     static std::atomic<unsigned long long> mask{0};
-    auto fn = cols_kernel<N, MODE, float2, ImgC, float2, FPB>;
+    auto fn = cols_kernel<N, MODE, InC, ImgC, float2, FPB>;
     cudaError_t e = ensure_smem_attr((const void*)fn, smem, &mask);
     if (e != cudaSuccess) return e;
     const int grid = (a.n_cols + FPB - 1) / FPB;
@@ -23,8 +23,13 @@ static cudaError_t fwd_dispatch(const ColArgs& a, cudaStream_t st) {
     return cols_impl<N, COL_FWD, float2>(a, st);
 }
 template <int N>
-static cudaError_t inv_dispatch(const ColArgs& a, cudaStream_t st) {
-    return cols_impl<N, COL_INV, float2>(a, st);
+static cudaError_t inv_dispatch(int in_dtype, const ColArgs& a, cudaStream_t st) {
+    switch (in_dtype) {
+        case 3: return cols_impl<N, COL_INV, float2, float2>(a, st);
+        case 4: return cols_impl<N, COL_INV, float2, __half2>(a, st);
+        case 5: return cols_impl<N, COL_INV, float2, __nv_bfloat162>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 template <int N>
 static cudaError_t xcorr_dispatch(int img_dtype, const ColArgs& a, cudaStream_t st) {
@@ -37,7 +42,9 @@ static cudaError_t xcorr_dispatch(int img_dtype, const ColArgs& a, cudaStream_t 
 }
 
 cudaError_t launch_cols_fwd(int n, const ColArgs& a, cudaStream_t st) { FFB_SIZE_SWITCH(n, fwd_dispatch, a, st) }
-cudaError_t launch_cols_inv(int n, const ColArgs& a, cudaStream_t st) { FFB_SIZE_SWITCH(n, inv_dispatch, a, st) }
+cudaError_t launch_cols_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st) {
+    FFB_SIZE_SWITCH(n, inv_dispatch, in_dtype, a, st)
+}
 cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st) {
     FFB_SIZE_SWITCH(n, xcorr_dispatch, img_dtype, a, st)
 }

@@ -41,6 +41,17 @@ struct fastfft_plan_s {
     size_t buffer_bytes = 0;
     long long pitch_a = 0, bytes_a = 0, pitch_b = 0, bytes_b = 0;
 
+    // Reduced-size correlation (2D, forward pad + inverse crop): with the template in
+    // [0, L) and the window in [0, W) per axis, every valid lag reads only image pixels
+    // [0, L + W - 1), so the size-N circular correlation equals a size-M one with
+    // M = pow2 >= L + W - 1, computed against the spectrum of the image cropped to
+    // [0, M) (prepared once per image, region C).
+    bool red_ok = false;
+    long long red_mx = 0, red_my = 0;
+    long long bytes_c = 0;     // prep work (max of the two column-major stages) + real crop + reduced spectrum
+    long long off_c_real = 0, off_c_spec = 0;
+    bool force_full_size = false;  // fastfft_set_full_size_correlation
+
     cudaStream_t stream = cudaStreamPerThread;
     std::string last_error;
 

@@ -154,6 +154,15 @@ class FourierTransformer:
         self._check(self._lib.fastfft_fwd_image_inv_many(self._h, n, ins, ims, outs, _opref(pre_op), _opref(intra_op),
                                                          _opref(post_op)))
 
+    def SetFullSizeCorrelation(self, force=True):
+        """Make FwdImageInvFFTMany use the size-N kernels even when a smaller size is exact."""
+        self._check(self._lib.fastfft_set_full_size_correlation(self._h, int(bool(force))))
+
+    def CorrelationSize(self):
+        d = (ctypes.c_int * 2)()
+        self._check(self._lib.fastfft_correlation_size(self._h, d))
+        return tuple(d)
+
     # -- accounting and profiling ------------------------------------------
     def LaunchCount(self):
         return self._ll(self._lib.fastfft_launch_count)

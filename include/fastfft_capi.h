@@ -115,6 +115,17 @@ FASTFFT_API fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, c
                                                       const fastfft_op* pre_op, const fastfft_op* intra_op,
                                                       const fastfft_op* post_op);
 
+/* The batched call correlates at the smallest power-of-two size M >= L + W - 1 per axis
+ * when that is below the plan's N (template in [0, L), window in [0, W)): every
+ * retained lag then reads image pixels in [0, L + W - 1) only, so the size-M
+ * circular correlation against the spectrum of the image cropped to [0, M) gives the
+ * same values as the size-N one.  Each distinct image in a call is prepared once.
+ * force != 0 selects the size-N kernels instead.  No reference counterpart (the
+ * reference aborts on a forward increase with an inverse decrease, FastFFT.cu:673-679). */
+FASTFFT_API fastfft_status fastfft_set_full_size_correlation(fastfft_handle h, int force);
+/* Transform size {x, y} that fastfft_fwd_image_inv_many uses for this plan. */
+FASTFFT_API fastfft_status fastfft_correlation_size(fastfft_handle h, int dims[2]);
+
 /* ReturnInputMemorySize / ReturnFwdOutputMemorySize / ReturnInvOutputMemorySize
  * (FastFFT.h:194-204): element counts of InputType, FFTW-padded. */
 FASTFFT_API fastfft_status fastfft_input_memory_size(fastfft_handle h, long long* n);
