@@ -1,0 +1,111 @@
+"""Batched correlation (fastfft_fwd_image_inv_many) against the FP64 oracle.
+
+The batched call correlates at the smallest exact size M = pow2 >= L + W - 1 per axis
+when M < N; these tests check that the retained window equals the size-N correlation
+the reference defines (FwdImageInvFFT, conj(T) * I, origin-anchored crop).
+"""
+import numpy as np
+import pytest
+
+import fastfft_b200 as F
+from oracle import fastfft_oracle as O
+from tests._util import RTOL_L2_FP32, RTOL_MAX_FP32, dev, empty, host
+
+pytestmark = pytest.mark.gpu
+
+
+def plan(fin, fout, iout, **kw):
+    ft = F.FourierTransformer(**kw)
+    ft.SetForwardFFTPlan(*fin, *fout)
+    ft.SetInverseFFTPlan(*fout, *iout)
+    return ft
+
+
+def image_spectrum(fout, seed):
+    img = np.random.default_rng(seed).standard_normal((fout[1], fout[0]))
+    return O.fwd(O.real_to_padded(img, fout, dtype=np.float64), fout, fout).astype(np.complex64)
+
+
+CASES = [
+    ((48, 48, 1), (512, 512, 1), (40, 40, 1), (128, 128)),
+    ((100, 60, 1), (1024, 512, 1), (130, 70, 1), (256, 256)),
+    ((128, 128, 1), (4096, 4096, 1), (512, 512, 1), (1024, 1024)),
+    ((256, 256, 1), (1024, 1024, 1), (512, 512, 1), (1024, 1024)),   # M = N: full size
+    ((33, 200, 1), (64, 2048, 1), (30, 100, 1), (64, 512)),
+]
+
+
+@pytest.mark.parametrize("fin,fout,iout,msize", CASES)
+def test_many_matches_oracle(torch_cuda, fin, fout, iout, msize):
+    torch = torch_cuda
+    ft = plan(fin, fout, iout)
+    assert ft.CorrelationSize() == msize
+    specs = [image_spectrum(fout, s) for s in (1, 2)]
+    d_specs = [dev(torch, s.view(np.float32)) for s in specs]
+    rng = np.random.default_rng(5)
+    ts = [rng.standard_normal((fin[1], fin[0])).astype(np.float32) for _ in range(5)]
+    which = [0, 1, 0, 0, 1]                      # interleaved images: grouping must keep pairs
+    ins = [dev(torch, O.real_to_padded(t, fin)) for t in ts]
+    outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    ft.FwdImageInvFFTMany(ins, [d_specs[w] for w in which], outs)
+    p = O.Plan(fin, fout, fout, iout)
+    for t, w, o in zip(ts, which, outs):
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), specs[w], p, out_dtype=np.float64), iout)
+        got = O.real_from_padded(host(o), iout)
+        assert O.rel_l2(got, ref) <= RTOL_L2_FP32
+        assert O.rel_max(got, ref) <= RTOL_MAX_FP32
+
+
+def test_many_equals_full_size_path(torch_cuda):
+    torch = torch_cuda
+    fin, fout, iout = (64, 64, 1), (1024, 1024, 1), (200, 200, 1)
+    spec = dev(torch, image_spectrum(fout, 9).view(np.float32))
+    t = dev(torch, O.real_to_padded(np.random.default_rng(3).standard_normal((64, 64)).astype(np.float32), fin))
+    a = plan(fin, fout, iout)
+    b = plan(fin, fout, iout)
+    b.SetFullSizeCorrelation(True)
+    assert a.CorrelationSize() == (512, 512) and b.CorrelationSize() == (1024, 1024)
+    oa, ob, oc = (empty(torch, a.ReturnInvOutputMemorySize(), torch.float32) for _ in range(3))
+    a.FwdImageInvFFTMany([t], spec, [oa])
+    b.FwdImageInvFFTMany([t], spec, [ob])
+    a.FwdImageInvFFT(t, spec, oc)                       # single call: size-N kernels
+    ra, rb, rc = (O.real_from_padded(host(x), iout) for x in (oa, ob, oc))
+    assert np.array_equal(rb, rc)
+    assert O.rel_l2(ra, rc) <= RTOL_L2_FP32
+
+
+def test_many_headline_shape_peak(torch_cuda):
+    """384^2 template, 4096^2 image (noise + blobs), 1024^2 window: computed at 2048^2."""
+    torch = torch_cuda
+    n, L, W = 4096, 384, 1024
+    spec = O.image_spectrum_fp32(O.gaussian_blob_image(n))
+    t = O.normal_template(L, O.SEED_BASE + 1).astype(np.float32)
+    fin, fout, iout = (L, L, 1), (n, n, 1), (W, W, 1)
+    ft = plan(fin, fout, iout)
+    assert ft.CorrelationSize() == (2048, 2048)
+    out = empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32)
+    ft.FwdImageInvFFTMany([dev(torch, O.real_to_padded(t, fin))], dev(torch, spec.view(np.float32)), [out])
+    got = O.real_from_padded(host(out), iout)[0]
+    p = O.Plan(fin, fout, fout, iout)
+    ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), spec, p, out_dtype=np.float64), iout)[0]
+    assert O.rel_l2(got, ref) <= RTOL_L2_FP32
+    gi, _, _ = O.peak(got)
+    ri, _, _ = O.peak(ref)
+    assert gi == ri
+
+
+@pytest.mark.parametrize("img_dt", ["complex32", "complex_bf16"])
+def test_many_low_precision_image(torch_cuda, img_dt):
+    torch = torch_cuda
+    fin, fout, iout = (96, 96, 1), (1024, 1024, 1), (256, 256, 1)
+    tdt = torch.float16 if img_dt == "complex32" else torch.bfloat16
+    spec = image_spectrum(fout, 4) / 1024
+    spec_q = torch.from_numpy(spec.view(np.float32).reshape(-1)).to(tdt)
+    spec_deq = spec_q.float().numpy().view(np.complex64).reshape(spec.shape)
+    ft = plan(fin, fout, iout, image_dtype=img_dt)
+    t = np.random.default_rng(8).standard_normal((96, 96)).astype(np.float32)
+    out = empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32)
+    ft.FwdImageInvFFTMany([dev(torch, O.real_to_padded(t, fin))], spec_q.cuda(), [out])
+    p = O.Plan(fin, fout, fout, iout)
+    ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), spec_deq, p, out_dtype=np.float64), iout)
+    assert O.rel_l2(O.real_from_padded(host(out), iout), ref) <= RTOL_L2_FP32
