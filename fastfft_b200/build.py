@@ -15,15 +15,15 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "libfastfft_b200.so"
-SOURCES = ["twiddles.cu", "launch_rows.cu", "launch_cols.cu", "capi.cu"]
+SOURCES = ["twiddles.cu", "launch_rows.cu", "launch_cols.cu", "launch_xcorr.cu", "capi.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr"]
 
 
-def _compile(src: str, extra: list[str]) -> tuple[str, str]:
-    out = OBJ / (Path(src).stem + ".o")
+def _compile(src: str, extra: list[str], obj_dir: Path = OBJ) -> tuple[str, str]:
+    out = obj_dir / (Path(src).stem + ".o")
     cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", str(CSRC / src), "-o", str(out)]
     p = subprocess.run(cmd, capture_output=True, text=True)
     if p.returncode != 0:
@@ -39,25 +39,30 @@ def _needs_build(extra: list[str]) -> bool:
     return any(d.stat().st_mtime > lib_t for d in deps if d.exists())
 
 
-def build(jobs: int | None = None, ptxas_verbose: bool = False, force: bool = False) -> Path:
+def build(jobs: int | None = None, ptxas_verbose: bool = False, force: bool = False,
+          defines: list[str] | None = None, out: Path | None = None) -> Path:
+    """Compile and link the library; `defines` (NAME=VALUE) and `out` build a variant elsewhere."""
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-    if not force and not ptxas_verbose and not _needs_build(extra):
+    extra += [f"-D{d}" for d in (defines or [])]
+    lib = Path(out) if out else LIB
+    if not force and not ptxas_verbose and not defines and out is None and not _needs_build(extra):
         return LIB
-    OBJ.mkdir(exist_ok=True)
+    obj_dir = OBJ if out is None else Path(out).parent / "_obj"
+    obj_dir.mkdir(parents=True, exist_ok=True)
     jobs = jobs or min(len(SOURCES), os.cpu_count() or 1)
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
-        results = list(ex.map(lambda s: _compile(s, extra), SOURCES))
+        results = list(ex.map(lambda s: _compile(s, extra, obj_dir), SOURCES))
     if ptxas_verbose:
         for _, log in results:
             sys.stderr.write(log)
     objs = [r[0] for r in results]
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = lib.with_suffix(".so.tmp")
     cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", str(tmp), "-lcudart"]
     p = subprocess.run(cmd, capture_output=True, text=True)
     if p.returncode != 0:
         raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{p.stdout}\n{p.stderr}")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
@@ -65,5 +70,7 @@ if __name__ == "__main__":
     ap.add_argument("--jobs", type=int, default=None)
     ap.add_argument("--ptxas-verbose", action="store_true")
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--define", action="append", default=[], help="NAME=VALUE preprocessor define")
+    ap.add_argument("--out", default=None, help="write the library here instead of in-tree")
     a = ap.parse_args()
-    print(build(a.jobs, a.ptxas_verbose, a.force))
+    print(build(a.jobs, a.ptxas_verbose, a.force, a.define, a.out))

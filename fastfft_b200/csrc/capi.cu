@@ -14,7 +14,7 @@
 #include <vector>
 
 #include "../../include/fastfft_capi.h"
-#include "kernels_2d.cuh"
+#include "kernels_xcorr.cuh"
 #include "launch.h"
 #include "plan.h"
 
@@ -141,14 +141,28 @@ void size_buffers(fastfft_plan_s* h) {
             const long long spec = (mx / 2 + 1) * my * 8;                                // reduced spectrum
             h->off_c_real = round_up(stage, 256);
             h->off_c_spec = h->off_c_real + round_up(real, 256);
-            h->bytes_c = h->off_c_spec + round_up(spec, 256);
+            // templates per launch: bounded by the shared memory of the fused column kernel
+            h->red_batch = ffb::kMaxBatch < 8 ? ffb::kMaxBatch : 8;
+            while (h->red_batch > 1 &&
+                   xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, h->red_batch) > 227 * 1024)
+                h->red_batch--;
+            if (xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, 1) > 227 * 1024) {
+                h->red_ok = false;
+                h->bytes_c = 0;
+                return;
+            }
+            h->red_t1_stride = round_up((mx / 2 + 1) * h->pitch_a, 32);   // complex elements per template
+            h->red_t2_stride = round_up((mx / 2 + 1) * h->pitch_b, 32);
+            h->off_c_t1 = h->off_c_spec + round_up(spec, 256);
+            h->off_c_t2 = h->off_c_t1 + h->red_batch * h->red_t1_stride * 8;
+            h->bytes_c = h->off_c_t2 + h->red_batch * h->red_t2_stride * 8;
         }
     }
 }
 
 fastfft_status allocate(fastfft_plan_s* h) {
     size_buffers(h);
-    const size_t need = (size_t)(h->bytes_a + h->bytes_b + h->bytes_c);
+    const size_t need = (size_t)(h->bytes_a + h->bytes_b + h->bytes_c) + 256;
     if (h->buffer && h->buffer_bytes >= need) return FASTFFT_OK;
     if (h->buffer) {
         cudaFree(h->buffer);
@@ -165,6 +179,9 @@ fastfft_status allocate(fastfft_plan_s* h) {
         return fail(h, FASTFFT_ERR_ALLOC, std::string("cudaMalloc of the work buffer failed: ") + cudaGetErrorString(e));
     }
     h->buffer_bytes = need;
+    h->dev_err = reinterpret_cast<int*>(static_cast<char*>(h->buffer) + need - 256);
+    e = cudaMemset(h->dev_err, 0, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemset of the status word");
     return FASTFFT_OK;
 }
 
@@ -219,7 +236,9 @@ fastfft_status run_fwd_rows(fastfft_plan_s* h, const void* in, float pre_scale, 
     cudaError_t e = twiddles_for(nx, &tw);
     if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     RowFwdArgs a;
-    a.in = in;
+    std::memset(&a, 0, sizeof(a));
+    a.in[0] = in;
+    a.n_batch = 1;
     a.in_pitch = 2LL * h->fwd_in.w;
     a.n_rows = (int)h->fwd_in.y;
     a.L = (int)h->fwd_in.x;
@@ -241,10 +260,12 @@ fastfft_status run_inv_rows(fastfft_plan_s* h, void* out, float post_scale) {
     cudaError_t e = twiddles_for(nx, &tw);
     if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     RowInvArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.n_batch = 1;
     a.in = region_b(h);
     a.in_pitch = h->pitch_b;
     a.n_rows = (int)h->inv_out.y;
-    a.out = out;
+    a.out[0] = out;
     a.out_pitch = 2LL * h->inv_out.w;
     a.W = (int)h->inv_out.x;
     a.scale = post_scale;
@@ -392,6 +413,7 @@ fastfft_status fastfft_fwd(fastfft_handle h, const void* input, void* output, co
     c.out_scale = 1.f;
     c.intra_scale = 1.f;
     c.tw = tw;
+    c.n_batch = 1;
     e = launch_cols_fwd(ny, c, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "forward column pass");
     h->launches++;
@@ -430,6 +452,7 @@ fastfft_status fastfft_inv(fastfft_handle h, const void* input, void* output, co
     c.out_scale = 1.f;
     c.intra_scale = 1.f;
     c.tw = tw;
+    c.n_batch = 1;
     e = launch_cols_inv(ny, FASTFFT_DTYPE_C64, c, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "inverse column pass");
     h->launches++;
@@ -480,6 +503,7 @@ static fastfft_status xcorr_one(fastfft_handle h, const void* input, const void*
     c.in_scale = 1.f;
     c.out_scale = 1.f;
     c.tw = tw;
+    c.n_batch = 1;
     e = launch_cols_xcorr(ny, h->image_dtype, c, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "cross-correlation column pass");
     h->launches++;
@@ -508,18 +532,22 @@ static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spec
     std::memset(&c1, 0, sizeof(c1));
     c1.in = image_spectrum; c1.in_stride = ny; c1.L = ny;
     c1.out = stage; c1.out_stride = my; c1.W = my; c1.n_cols = nx / 2 + 1;
-    c1.in_scale = 1.f; c1.out_scale = 1.f; c1.intra_scale = 1.f; c1.tw = tw;
+    c1.in_scale = 1.f; c1.out_scale = 1.f; c1.intra_scale = 1.f; c1.tw = tw; c1.n_batch = 1;
     if ((e = launch_cols_inv(ny, h->image_dtype, c1, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (inverse columns)");
     // 2. C2R along x, keep x < Mx: crop[y][x]
     if ((e = twiddles_for(nx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     RowInvArgs r2;
-    r2.in = stage; r2.in_pitch = my; r2.n_rows = my; r2.out = crop; r2.out_pitch = crop_pitch; r2.W = mx;
+    std::memset(&r2, 0, sizeof(r2));
+    r2.n_batch = 1;
+    r2.in = stage; r2.in_pitch = my; r2.n_rows = my; r2.out[0] = crop; r2.out_pitch = crop_pitch; r2.W = mx;
     r2.scale = 1.f; r2.tw = tw;
     if ((e = launch_c2r_rows(nx, FASTFFT_DTYPE_F32, r2, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (C2R rows)");
     // 3. R2C along x at size Mx: stage[kx][y]
     if ((e = twiddles_for(mx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     RowFwdArgs r3;
-    r3.in = crop; r3.in_pitch = crop_pitch; r3.n_rows = my; r3.L = mx; r3.out = stage; r3.out_pitch = my;
+    std::memset(&r3, 0, sizeof(r3));
+    r3.n_batch = 1;
+    r3.in[0] = crop; r3.in_pitch = crop_pitch; r3.n_rows = my; r3.L = mx; r3.out = stage; r3.out_pitch = my;
     r3.kmax = mx / 2 + 1; r3.scale = 1.f; r3.tw = tw;
     if ((e = launch_r2c_rows(mx, FASTFFT_DTYPE_F32, r3, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (R2C rows)");
     // 4. forward along y at size My, scaled: spec[kx][ky]
@@ -528,44 +556,57 @@ static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spec
     std::memset(&c4, 0, sizeof(c4));
     c4.in = stage; c4.in_stride = my; c4.L = my;
     c4.out = spec; c4.out_stride = my; c4.W = my; c4.n_cols = mx / 2 + 1;
-    c4.in_scale = 1.f; c4.out_scale = 1.f / ((float)mx * (float)my); c4.intra_scale = 1.f; c4.tw = tw;
+    c4.in_scale = 1.f; c4.out_scale = 1.f / ((float)mx * (float)my); c4.intra_scale = 1.f; c4.tw = tw; c4.n_batch = 1;
     if ((e = launch_cols_fwd(my, c4, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (forward columns)");
     h->launches += 4;
     return FASTFFT_OK;
 }
 
-// One template through the reduced-size correlation against the prepared spectrum.
-static fastfft_status red_xcorr_one(fastfft_handle h, const void* input, void* out, const fastfft_op* pre_op,
-                                    const fastfft_op* intra_op, const fastfft_op* post_op) {
+// Up to kMaxBatch templates through the reduced-size correlation against the prepared
+// spectrum: three launches whose grid.y runs over the templates.
+static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const* inputs, void* const* outs,
+                                      const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                      const fastfft_op* post_op) {
     const int mx = (int)h->red_mx, my = (int)h->red_my;
-    const float2* spec = reinterpret_cast<const float2*>(region_c(h) + h->off_c_spec);
+    char* c0 = region_c(h);
+    const float2* spec = reinterpret_cast<const float2*>(c0 + h->off_c_spec);
+    float2* t1 = reinterpret_cast<float2*>(c0 + h->off_c_t1);
+    float2* t2 = reinterpret_cast<float2*>(c0 + h->off_c_t2);
     const float2* tw = nullptr;
     cudaError_t e;
     prof_begin_call(h);
     if ((e = twiddles_for(mx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     RowFwdArgs a;
-    a.in = input; a.in_pitch = 2LL * h->fwd_in.w; a.n_rows = (int)h->fwd_in.y; a.L = (int)h->fwd_in.x;
-    a.out = region_a(h); a.out_pitch = h->pitch_a; a.kmax = mx / 2 + 1; a.scale = scale_of(pre_op); a.tw = tw;
+    std::memset(&a, 0, sizeof(a));
+    for (int g = 0; g < n; g++) a.in[g] = inputs[g];
+    a.n_batch = n;
+    a.in_pitch = 2LL * h->fwd_in.w; a.n_rows = (int)h->fwd_in.y; a.L = (int)h->fwd_in.x;
+    a.out = t1; a.out_pitch = h->pitch_a; a.out_batch_stride = h->red_t1_stride;
+    a.kmax = mx / 2 + 1; a.scale = scale_of(pre_op); a.tw = tw;
     if ((e = launch_r2c_rows(mx, h->input_dtype, a, h->stream)) != cudaSuccess) return cuda_fail(h, e, "r2c row pass");
     h->launches++;
     prof_mark(h);
     if ((e = twiddles_for(my, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
-    ColArgs c;
+    XcorrColArgs c;
     std::memset(&c, 0, sizeof(c));
-    c.in = region_a(h); c.in_stride = h->pitch_a; c.L = (int)h->fwd_in.y;
+    c.t1 = t1; c.t1_pitch = h->pitch_a; c.t1_batch = h->red_t1_stride; c.L = (int)h->fwd_in.y;
     c.img = spec; c.img_stride = my;
-    c.out = region_b(h); c.out_stride = h->pitch_b; c.W = (int)h->inv_out.y; c.n_cols = mx / 2 + 1;
+    c.out = t2; c.out_pitch = h->pitch_b; c.out_batch = h->red_t2_stride; c.W = (int)h->inv_out.y;
+    c.n_cols = mx / 2 + 1; c.n_batch = n;
     c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
     c.intra_scale = intra_op ? intra_op->scale : 1.f;
-    c.in_scale = 1.f; c.out_scale = 1.f; c.tw = tw;
-    if ((e = launch_cols_xcorr(my, FASTFFT_DTYPE_C64, c, h->stream)) != cudaSuccess)
+    c.tw = tw; c.err = h->dev_err;
+    if ((e = launch_xcorr_cols(my, FASTFFT_DTYPE_C64, c, h->stream)) != cudaSuccess)
         return cuda_fail(h, e, "cross-correlation column pass");
     h->launches++;
     prof_mark(h);
     if ((e = twiddles_for(mx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     RowInvArgs r;
-    r.in = region_b(h); r.in_pitch = h->pitch_b; r.n_rows = (int)h->inv_out.y;
-    r.out = out; r.out_pitch = 2LL * h->inv_out.w; r.W = (int)h->inv_out.x; r.scale = scale_of(post_op); r.tw = tw;
+    std::memset(&r, 0, sizeof(r));
+    r.n_batch = n;
+    r.in = t2; r.in_pitch = h->pitch_b; r.in_batch_stride = h->red_t2_stride; r.n_rows = (int)h->inv_out.y;
+    for (int g = 0; g < n; g++) r.out[g] = outs[g];
+    r.out_pitch = 2LL * h->inv_out.w; r.W = (int)h->inv_out.x; r.scale = scale_of(post_op); r.tw = tw;
     if ((e = launch_c2r_rows(mx, h->output_dtype, r, h->stream)) != cudaSuccess) return cuda_fail(h, e, "c2r row pass");
     h->launches++;
     prof_mark(h);
@@ -606,17 +647,28 @@ fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, const void* c
     // Reduced-size path: templates are grouped by image (in order of first use); each
     // distinct image is prepared once for the whole call.
     std::vector<char> done(n, 0);
+    const void* grp_in[kMaxBatch];
+    void* grp_out[kMaxBatch];
     for (int i = 0; i < n; i++) {
         if (done[i]) continue;
         const void* img = image_spectra[i];
         st = red_prepare_image(h, img);
         if (st != FASTFFT_OK) return st;
+        int m = 0;
         for (int k = i; k < n; k++) {
             if (done[k] || image_spectra[k] != img) continue;
-            void* out = (outputs && outputs[k]) ? outputs[k] : const_cast<void*>(inputs[k]);
-            st = red_xcorr_one(h, inputs[k], out, pre_op, intra_op, post_op);
-            if (st != FASTFFT_OK) return st;
+            grp_in[m] = inputs[k];
+            grp_out[m] = (outputs && outputs[k]) ? outputs[k] : const_cast<void*>(inputs[k]);
             done[k] = 1;
+            if (++m == h->red_batch) {
+                st = red_xcorr_batch(h, m, grp_in, grp_out, pre_op, intra_op, post_op);
+                if (st != FASTFFT_OK) return st;
+                m = 0;
+            }
+        }
+        if (m > 0) {
+            st = red_xcorr_batch(h, m, grp_in, grp_out, pre_op, intra_op, post_op);
+            if (st != FASTFFT_OK) return st;
         }
     }
     return FASTFFT_OK;
@@ -731,6 +783,15 @@ fastfft_status fastfft_wait(fastfft_handle h) {
     if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamSynchronize");
+    if (h->dev_err) {
+        int flag = 0;
+        e = cudaMemcpy(&flag, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(h, e, "reading the status word");
+        if (flag) {
+            cudaMemset(h->dev_err, 0, sizeof(int));
+            return fail(h, FASTFFT_ERR_TIMEOUT, "a kernel gave up waiting for its bulk copies; its outputs are incomplete");
+        }
+    }
     return FASTFFT_OK;
 }
 

@@ -205,32 +205,24 @@ __device__ __forceinline__ void dft16(float2 (&v)[16]) {
 }
 
 // DFT16 when only v[q], q < qnz, can be non-zero (forward size increase: the
-// zero-padded tail of a column is never loaded or transformed).
+// zero-padded tail of a column is never loaded or transformed).  Only the first
+// stage (DFT4 over n2) is specialised, so the three variants share one register
+// allocation for the twiddle and outer stages.
 template <bool INV>
 __device__ __forceinline__ void dft16_pruned(float2 (&v)[16], int qnz) {
-    if (qnz >= 16 || qnz > 8) {
-        dft16<INV>(v);
-        return;
-    }
-    if (qnz <= 1) {
-        float2 x0 = v[0];
-#pragma unroll
-        for (int k = 0; k < 16; k++) v[k] = x0;
-        return;
-    }
     float2 a[16];
     if (qnz <= 4) {
-        // n2 = 0 only: the first-stage DFT4s are copies
+        // only n2 = 0: the first-stage DFT4s are copies
 #pragma unroll
         for (int n1 = 0; n1 < 4; n1++) {
-            float2 x = v[n1];
+            const float2 x = v[n1];
             a[n1] = x; a[n1 + 4] = x; a[n1 + 8] = x; a[n1 + 12] = x;
         }
-    } else {
+    } else if (qnz <= 8) {
         // n2 in {0, 1}: DFT4 of (x0, x1, 0, 0) = (x0 + x1, x0 -+ i x1, x0 - x1, x0 +- i x1)
 #pragma unroll
         for (int n1 = 0; n1 < 4; n1++) {
-            float2 x0 = v[n1], x1 = v[n1 + 4];
+            const float2 x0 = v[n1], x1 = v[n1 + 4];
             a[n1] = cadd(x0, x1);
             a[n1 + 8] = csub(x0, x1);
             if (!INV) {
@@ -241,6 +233,13 @@ __device__ __forceinline__ void dft16_pruned(float2 (&v)[16], int qnz) {
                 a[n1 + 12] = make_float2(x0.x + x1.y, x0.y - x1.x);
             }
         }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 16; i++) a[i] = v[i];
+        dft4<INV>(a[0], a[4], a[8], a[12]);
+        dft4<INV>(a[1], a[5], a[9], a[13]);
+        dft4<INV>(a[2], a[6], a[10], a[14]);
+        dft4<INV>(a[3], a[7], a[11], a[15]);
     }
     dft16_inner_twiddles<INV>(a);
     dft16_outer<INV>(a, v);
@@ -294,6 +293,45 @@ __device__ __forceinline__ int phys(int i) { return i + (i >> 4); }
 //   tw[off + r*Ns + t] = exp(-2 pi i r t / (16 Ns)),  r < 16, t < Ns.
 // Generated in FP64 (sincospi) and rounded to FP32 once.
 
+// Twiddle-table load that the compiler may not hoist out of loops: keeping the
+// table values of every pass live across a loop over transforms would double the
+// register demand of the fused kernels.
+__device__ __forceinline__ float2 ld_tw(const float2* p) {
+    float2 r;
+    asm volatile("ld.global.nc.v2.f32 {%0, %1}, [%2];" : "=f"(r.x), "=f"(r.y) : "l"(p));
+    return r;
+}
+
+// Radix-16 pass twiddles v[r] *= W^(r t), r = 1..15, from the four table values
+// W^t, W^2t, W^4t, W^8t; the other eleven are products of at most three table values
+// (for t = 0 all are exactly 1).  Four loads per pass instead of fifteen keeps the
+// shared L1/shared-memory data path, the binding unit of these kernels, free for the
+// exchanges.
+template <bool INV>
+__device__ __forceinline__ void twiddle_pass(float2 (&v)[16], float2 w1, float2 w2, float2 w4, float2 w8) {
+#define FFB_TWMUL(r, w) v[r] = INV ? cmulc(v[r], (w)) : cmul(v[r], (w))
+    const float2 w3 = cmul(w1, w2);
+    FFB_TWMUL(1, w1);
+    FFB_TWMUL(2, w2);
+    FFB_TWMUL(3, w3);
+    FFB_TWMUL(4, w4);
+    const float2 w5 = cmul(w1, w4);
+    FFB_TWMUL(5, w5);
+    const float2 w6 = cmul(w2, w4);
+    FFB_TWMUL(6, w6);
+    const float2 w7 = cmul(w3, w4);
+    FFB_TWMUL(7, w7);
+    FFB_TWMUL(8, w8);
+    FFB_TWMUL(9, cmul(w1, w8));
+    FFB_TWMUL(10, cmul(w2, w8));
+    FFB_TWMUL(11, cmul(w3, w8));
+    FFB_TWMUL(12, cmul(w4, w8));
+    FFB_TWMUL(13, cmul(w5, w8));
+    FFB_TWMUL(14, cmul(w6, w8));
+    FFB_TWMUL(15, cmul(w7, w8));
+#undef FFB_TWMUL
+}
+
 template <int N, bool INV>
 struct BlockFft {
     using S = FftShape<N>;
@@ -325,11 +363,7 @@ struct BlockFft {
             const int ns = S::REM << (4 * p);
             if (ns > 1) {
                 const float2* __restrict__ t = tw + S::tw_pass_offset(p) + (j & (ns - 1));
-#pragma unroll
-                for (int r = 1; r < 16; r++) {
-                    const float2 w = __ldg(t + r * ns);
-                    v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
-                }
+                twiddle_pass<INV>(v, ld_tw(t + ns), ld_tw(t + 2 * ns), ld_tw(t + 4 * ns), ld_tw(t + 8 * ns));
             }
             if (S::REM == 1 && p == 0)
                 dft16_pruned<INV>(v, qnz);

@@ -72,9 +72,13 @@ __device__ __forceinline__ int leading_slots(int L, int j) {
 // ---------------------------------------------------------------------------
 // Row R2C (forward), two rows per complex FFT
 // ---------------------------------------------------------------------------
+// Templates per launch: blockIdx.y selects the template of a batch.
+constexpr int kMaxBatch = 16;
+
 struct RowFwdArgs {
-    const void* in;        // real rows, row r at in + r * in_pitch (elements)
+    const void* in[kMaxBatch];  // real rows of template g: row r at in[g] + r * in_pitch (elements)
     long long in_pitch;
+    long long out_batch_stride; // complex elements between the outputs of consecutive templates
     int n_rows;            // rows that exist (rows >= n_rows are not produced)
     int L;                 // valid x per row; x in [L, N) is zero padding
     float2* out;           // out[k * out_pitch + r] for k < kmax
@@ -82,6 +86,7 @@ struct RowFwdArgs {
     int kmax;              // kx outputs written (N/2+1, or fewer for a decrease)
     float scale;           // pre-op SCALE (1 = NOOP)
     const float2* tw;      // twiddle table of size N
+    int n_batch;           // templates in this launch (grid.y)
 };
 
 template <int N, class InT, int FPB>
@@ -95,7 +100,8 @@ r2c_rows_kernel(RowFwdArgs a) {
     float2* s = smem + f * S::SMEM;
     const int ra = 2 * (blockIdx.x * FPB + f);
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
-    const InT* pa = static_cast<const InT*>(a.in) + (long long)ra * a.in_pitch;
+    const InT* pa = static_cast<const InT*>(a.in[blockIdx.y]) + (long long)ra * a.in_pitch;
+    float2* const out_g = a.out + (long long)blockIdx.y * a.out_batch_stride;
     const InT* pb = pa + a.in_pitch;
     float2 v[16];
 #pragma unroll
@@ -126,7 +132,7 @@ r2c_rows_kernel(RowFwdArgs a) {
         const float2 A = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
         const float2 B = make_float2(0.5f * (z1.y + z2.y), 0.5f * (z2.x - z1.x));
         const int rr = 2 * (blockIdx.x * FPB + ff);
-        float2* o = a.out + (long long)k * a.out_pitch + rr;
+        float2* o = out_g + (long long)k * a.out_pitch + rr;
         if (rr + 1 < a.n_rows) {
             *reinterpret_cast<float4*>(o) = make_float4(A.x, A.y, B.x, B.y);
         } else if (rr < a.n_rows) {
@@ -141,8 +147,11 @@ r2c_rows_kernel(RowFwdArgs a) {
 enum ColMode { COL_FWD = 0, COL_INV = 1, COL_XCORR = 2 };
 
 struct ColArgs {
-    const void* in;          // column c at in + c * in_stride (complex elements)
+    const void* in;          // column c of batch entry g at in + g * in_batch_stride + c * in_stride
     long long in_stride;
+    long long in_batch_stride;
+    long long img_batch_stride;  // 0: every batch entry searches the same image
+    long long out_batch_stride;
     int L;                   // valid input rows per column (zero beyond)
     const void* img;         // XCORR: image spectrum column c at img + c * img_stride
     long long img_stride;
@@ -155,6 +164,7 @@ struct ColArgs {
     float in_scale;
     float out_scale;
     const float2* tw;
+    int n_batch;             // batch entries in this launch (grid.y)
 };
 
 template <int N, int MODE, class InC, class ImgC, class OutC, int FPB>
@@ -168,7 +178,8 @@ cols_kernel(ColArgs a) {
     float2* s = smem + f * S::SMEM;
     const int col = blockIdx.x * FPB + f;
     const bool valid = col < a.n_cols;
-    const InC* pin = static_cast<const InC*>(a.in) + (long long)col * a.in_stride;
+    const long long g = blockIdx.y;
+    const InC* pin = static_cast<const InC*>(a.in) + g * a.in_batch_stride + (long long)col * a.in_stride;
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
@@ -185,7 +196,7 @@ cols_kernel(ColArgs a) {
     }
     if constexpr (MODE == COL_XCORR) {
         if (a.intra_kind != 0) {
-            const ImgC* pimg = static_cast<const ImgC*>(a.img) + (long long)col * a.img_stride;
+            const ImgC* pimg = static_cast<const ImgC*>(a.img) + g * a.img_batch_stride + (long long)col * a.img_stride;
             const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
 #pragma unroll
             for (int q = 0; q < 16; q++) {
@@ -198,7 +209,7 @@ cols_kernel(ColArgs a) {
         BlockFft<N, true>::run(v, s, j, a.tw, 16);
     }
     if (valid) {
-        OutC* pout = static_cast<OutC*>(a.out) + (long long)col * a.out_stride;
+        OutC* pout = static_cast<OutC*>(a.out) + g * a.out_batch_stride + (long long)col * a.out_stride;
 #pragma unroll
         for (int q = 0; q < 16; q++) {
             const int n = j + T * q;
@@ -214,14 +225,16 @@ cols_kernel(ColArgs a) {
 // Row C2R (inverse), two rows per complex FFT
 // ---------------------------------------------------------------------------
 struct RowInvArgs {
-    const float2* in;      // in[k * in_pitch + r], k in [0, N/2], r < n_rows
+    const float2* in;      // batch entry g: in[g * in_batch_stride + k * in_pitch + r], k in [0, N/2], r < n_rows
     long long in_pitch;    // even
+    long long in_batch_stride;
     int n_rows;
-    void* out;             // real rows, row r at out + r * out_pitch (elements)
+    void* out[kMaxBatch];  // real rows of batch entry g: row r at out[g] + r * out_pitch (elements)
     long long out_pitch;
     int W;                 // x outputs kept per row
     float scale;           // post-op SCALE (1 = NOOP)
     const float2* tw;
+    int n_batch;           // batch entries in this launch (grid.y)
 };
 
 template <int N, class OutT, int FPB>
@@ -243,7 +256,7 @@ c2r_rows_kernel(RowInvArgs a) {
         const int k = i / FPB;
         const int rr = 2 * (blockIdx.x * FPB + ff);
         float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
-        const float2* p = a.in + (long long)k * a.in_pitch + rr;
+        const float2* p = a.in + (long long)blockIdx.y * a.in_batch_stride + (long long)k * a.in_pitch + rr;
         if (rr + 1 < a.n_rows) {
             const float4 t = *reinterpret_cast<const float4*>(p);
             A = make_float2(t.x, t.y);
@@ -265,7 +278,7 @@ c2r_rows_kernel(RowInvArgs a) {
     for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
     BlockFft<N, true>::run(v, s, j, a.tw, 16);
     const int ra = 2 * (blockIdx.x * FPB + f);
-    OutT* oa = static_cast<OutT*>(a.out) + (long long)ra * a.out_pitch;
+    OutT* oa = static_cast<OutT*>(a.out[blockIdx.y]) + (long long)ra * a.out_pitch;
     OutT* ob = oa + a.out_pitch;
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
 #pragma unroll

@@ -1,0 +1,178 @@
+// Fused cross-correlation column pass, batched over templates (sm_100a).
+//
+// One block per spectrum column kx serves every template of the batch:
+//   - the image-spectrum column (N values) and the template row-pass columns (L values
+//     per template) are brought into shared memory by TMA bulk copies
+//     (cp.async.bulk ... mbarrier::complete_tx) issued by one thread, so the image
+//     column is read once per batch instead of once per template;
+//   - each FFT group of the block then runs, per template, the zero-padded forward
+//     column FFT, the conj(T) * I intra-op against the shared image column, and the
+//     inverse FFT, and stores the first W outputs;
+// Replaces block_fft_kernel_C2C_FWD_INCREASE_OP_INV_NONE (src/fastfft/FastFFT.cu:20-56),
+// which reloads the image column per template and zero-pads explicitly.
+//
+// The mbarrier wait is bounded: if the copies have not landed after kWaitLimit polls,
+// the block records kErrTimeout in *err and returns without touching the outputs.
+#pragma once
+
+#include "kernels_2d.cuh"
+
+namespace ffb {
+
+constexpr int kErrTimeout = 1;
+constexpr long long kWaitLimit = 1ll << 26;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bulk global -> shared copy of `bytes` (multiple of 16; both addresses 16-byte aligned),
+// completion counted on `bar`.  No multicast.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Polls the barrier phase; returns false if it did not complete within the limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+    const uint32_t a = smem_addr(bar);
+    for (long long i = 0; i < kWaitLimit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+struct XcorrColArgs {
+    const float2* t1;          // template g, column c: t1 + g * t1_batch + c * t1_pitch (L valid values)
+    long long t1_pitch;
+    long long t1_batch;
+    int L;
+    const void* img;           // image column c: img + c * img_stride (ImgC elements)
+    long long img_stride;
+    float2* out;               // template g, column c: out + g * out_batch + c * out_pitch (W values)
+    long long out_pitch;
+    long long out_batch;
+    int W;
+    int n_cols;
+    int n_batch;
+    int intra_kind;            // 0 NOOP, 2 CONJ_MUL, 3 CONJ_MUL_THEN_SCALE
+    float intra_scale;
+    const float2* tw;
+    int* err;
+};
+
+// Shared-memory plan of the kernel (bytes), shared by the host launcher.
+template <int N, class ImgC, int FPB>
+struct XcorrSmem {
+    static constexpr int kImgBytes = N * (int)sizeof(ImgC);
+    static constexpr int kXchBytes = FPB * FftShape<N>::SMEM * (int)sizeof(float2);
+    static __host__ __device__ constexpr int t1_col_elems(int L) { return (L + 1) & ~1; }  // 16-byte multiple
+    static __host__ __device__ constexpr int img_off() { return 0; }
+    static __host__ __device__ constexpr int xch_off() { return (kImgBytes + 127) & ~127; }
+    static __host__ __device__ constexpr int t1_off() { return xch_off() + kXchBytes; }
+    static __host__ __device__ constexpr int bar_off(int L, int nb) {
+        return (t1_off() + nb * t1_col_elems(L) * 8 + 15) & ~15;
+    }
+    static __host__ __device__ constexpr int total(int L, int nb) { return bar_off(L, nb) + 16; }
+};
+
+#ifndef FFB_XCORR_MIN_BLOCKS
+#define FFB_XCORR_MIN_BLOCKS 2
+#endif
+
+template <int N, class ImgC, int FPB>
+__global__ void __launch_bounds__(FftShape<N>::T * FPB, FFB_XCORR_MIN_BLOCKS)
+xcorr_cols_kernel(XcorrColArgs a) {
+    using S = FftShape<N>;
+    using SM = XcorrSmem<N, ImgC, FPB>;
+    constexpr int T = S::T;
+    extern __shared__ __align__(128) unsigned char sm_raw[];
+    const ImgC* img_s = reinterpret_cast<const ImgC*>(sm_raw + SM::img_off());
+    float2* xch = reinterpret_cast<float2*>(sm_raw + SM::xch_off());
+    float2* t1_s = reinterpret_cast<float2*>(sm_raw + SM::t1_off());
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm_raw + SM::bar_off(a.L, a.n_batch));
+
+    const int col = blockIdx.x;
+    const int f = threadIdx.x / T;
+    const int j = threadIdx.x - f * T;
+    const int lcol = SM::t1_col_elems(a.L);
+
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+        const uint32_t bytes = (uint32_t)(SM::kImgBytes + a.n_batch * lcol * 8);
+        mbar_arrive_expect_tx(bar, bytes);
+        bulk_g2s(sm_raw + SM::img_off(), static_cast<const ImgC*>(a.img) + (long long)col * a.img_stride,
+                 SM::kImgBytes, bar);
+        for (int g = 0; g < a.n_batch; g++)
+            bulk_g2s(t1_s + g * lcol, a.t1 + g * a.t1_batch + (long long)col * a.t1_pitch, lcol * 8, bar);
+    }
+    __syncthreads();  // barrier initialised before anyone polls it
+    if (!mbar_wait(bar, 0)) {
+        if (threadIdx.x == 0) atomicExch(a.err, kErrTimeout);
+        // give the copies a second bounded chance to land before the block exits
+        mbar_wait(bar, 0);
+        return;
+    }
+
+    const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
+    const int rounds = (a.n_batch + FPB - 1) / FPB;
+    float2* s = xch + f * S::SMEM;
+#pragma unroll 1
+    for (int it = 0; it < rounds; it++) {
+        const int g = it * FPB + f;
+        const bool live = g < a.n_batch;
+        float2 v[16];
+        const float2* src = t1_s + (live ? g : 0) * lcol;
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int n = j + T * q;
+            v[q] = (live && n < a.L) ? src[n] : make_float2(0.f, 0.f);
+        }
+        BlockFft<N, false>::run(v, s, j, a.tw, live ? leading_slots<T>(a.L, j) : 0);
+        if (a.intra_kind != 0) {
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const float2 im = ld_cplx<ImgC>(img_s + j + T * q);
+                const float2 p = conj_mul(v[q], im);
+                v[q] = (sc != 1.f) ? cscale(p, sc) : p;
+            }
+        }
+        BlockFft<N, true>::run(v, s, j, a.tw, 16);
+        if (live) {
+            float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const int n = j + T * q;
+                if (n < a.W) o[n] = v[q];
+            }
+        }
+    }
+}
+
+}  // namespace ffb

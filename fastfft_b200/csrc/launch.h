@@ -12,6 +12,7 @@ namespace ffb {
 struct RowFwdArgs;
 struct ColArgs;
 struct RowInvArgs;
+struct XcorrColArgs;
 
 // dtype codes follow fastfft_dtype in include/fastfft_capi.h
 cudaError_t launch_r2c_rows(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
@@ -19,6 +20,9 @@ cudaError_t launch_c2r_rows(int n, int out_dtype, const RowInvArgs& a, cudaStrea
 cudaError_t launch_cols_fwd(int n, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st);
+// Batched fused column pass (TMA-staged image and template columns), n <= 4096.
+cudaError_t launch_xcorr_cols(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st);
+size_t xcorr_cols_smem(int n, int img_dtype, int L, int n_batch);
 
 // Device-wide FP64-generated twiddle table (generated once per device).
 cudaError_t twiddles_for(int n, const float2** out);

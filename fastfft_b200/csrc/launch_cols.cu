@@ -14,7 +14,8 @@ static cudaError_t cols_impl(const ColArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     const int grid = (a.n_cols + FPB - 1) / FPB;
     if (grid == 0) return cudaSuccess;
-    fn<<<grid, THREADS, smem, st>>>(a);
+    if (a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
+    fn<<<dim3(grid, a.n_batch), THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 

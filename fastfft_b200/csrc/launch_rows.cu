@@ -14,7 +14,8 @@ static cudaError_t r2c_impl(const RowFwdArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     const int grid = (a.n_rows + 2 * FPB - 1) / (2 * FPB);
     if (grid == 0) return cudaSuccess;
-    fn<<<grid, THREADS, smem, st>>>(a);
+    if (a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
+    fn<<<dim3(grid, a.n_batch), THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -43,7 +44,8 @@ static cudaError_t c2r_impl(const RowInvArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     const int grid = (a.n_rows + 2 * FPB - 1) / (2 * FPB);
     if (grid == 0) return cudaSuccess;
-    fn<<<grid, THREADS, smem, st>>>(a);
+    if (a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
+    fn<<<dim3(grid, a.n_batch), THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -1,0 +1,51 @@
+// Launcher for the batched fused correlation column pass (kernels_xcorr.cuh).
+#include "kernels_xcorr.cuh"
+#include "launch_common.cuh"
+
+namespace ffb {
+
+constexpr int kMaxDynSmem = 227 * 1024;
+
+template <int N, class ImgC>
+static cudaError_t xcorr_v2_impl(const XcorrColArgs& a, cudaStream_t st) {
+    if constexpr (N > 4096) {
+        return cudaErrorInvalidValue;
+    } else {
+        constexpr int FPB = col_fpb<N>();
+        using SM = XcorrSmem<N, ImgC, FPB>;
+        if (a.n_batch < 1 || a.n_batch > kMaxBatch || a.n_cols < 1) return cudaErrorInvalidValue;
+        const int smem = SM::total(a.L, a.n_batch);
+        if (smem > kMaxDynSmem) return cudaErrorInvalidValue;
+        static std::atomic<unsigned long long> mask{0};
+        auto fn = xcorr_cols_kernel<N, ImgC, FPB>;
+        cudaError_t e = ensure_smem_attr((const void*)fn, kMaxDynSmem, &mask);
+        if (e != cudaSuccess) return e;
+        fn<<<a.n_cols, FftShape<N>::T * FPB, smem, st>>>(a);
+        return cudaGetLastError();
+    }
+}
+
+template <int N>
+static cudaError_t xcorr_v2_dispatch(int img_dtype, const XcorrColArgs& a, cudaStream_t st) {
+    switch (img_dtype) {
+        case 3: return xcorr_v2_impl<N, float2>(a, st);
+        case 4: return xcorr_v2_impl<N, __half2>(a, st);
+        case 5: return xcorr_v2_impl<N, __nv_bfloat162>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_xcorr_cols(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st) {
+    FFB_SIZE_SWITCH(n, xcorr_v2_dispatch, img_dtype, a, st)
+}
+
+size_t xcorr_cols_smem(int n, int img_dtype, int L, int n_batch) {
+    const int isz = img_dtype == 3 ? 8 : 4;
+    const int fpb = (n / 16) >= 256 ? 1 : 256 / (n / 16);
+    const size_t img = ((size_t)n * isz + 127) & ~(size_t)127;
+    const size_t xch = (size_t)fpb * (n + n / 16) * 8;
+    const size_t t1 = (size_t)n_batch * (size_t)((L + 1) & ~1) * 8;
+    return ((img + xch + t1 + 15) & ~(size_t)15) + 16;
+}
+
+}  // namespace ffb
