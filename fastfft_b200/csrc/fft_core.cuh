@@ -19,7 +19,7 @@
 #include <stdint.h>
 
 #ifndef FFB_PACKED_F32X2
-#define FFB_PACKED_F32X2 1
+#define FFB_PACKED_F32X2 0
 #endif
 
 namespace ffb {
@@ -27,8 +27,9 @@ namespace ffb {
 constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
 
 // ---------------------------------------------------------------------------
-// Complex arithmetic on float2.  Component-aligned adds use the sm_100 paired
-// FP32 instructions (one instruction for both lanes of a complex number).
+// Complex arithmetic on float2.  FFB_PACKED_F32X2=1 maps the component-aligned adds
+// to the sm_100 paired FP32 instructions; measured on B200 it made the column passes
+// slower (register-pair moves), so the scalar form is the default.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) {
 #if FFB_PACKED_F32X2
@@ -256,6 +257,10 @@ struct FftShape {
     static constexpr int REM = 1 << (LOG & 3);   // radix of the optional first pass
     static constexpr int NP16 = LOG >> 2;        // number of radix-16 passes
     static constexpr int SMEM = N + N / 16;      // float2 per FFT exchange buffer
+    // Stride between the buffers of consecutive FFT groups of a block: 4 float2 past a
+    // multiple of 16, so that accesses that walk across groups (the row kernels' split
+    // and gather phases) land in different banks.
+    static constexpr int SMEM_PAD = ((SMEM + 15) / 16) * 16 + 4;
     // twiddle entries: for every radix-16 pass with stride Ns > 1, 16*Ns entries
     static constexpr int tw_pass_offset(int p) {
         int off = 0;
@@ -332,29 +337,69 @@ __device__ __forceinline__ void twiddle_pass(float2 (&v)[16], float2 w1, float2 
 #undef FFB_TWMUL
 }
 
+// Exchange buffers and barrier of one FFT group (T = N/16 threads) inside a block of
+// FPB groups.  Groups of at least one warp synchronise on their own named barrier
+// (bar.sync 1 + f, T), so the groups of a block do not wait for each other; smaller
+// groups fall back to __syncthreads().  With DB (double buffering) consecutive
+// exchanges alternate between two buffers, which makes the write-after-read barrier
+// unnecessary: a buffer is rewritten only after a barrier that every thread reaches
+// after its last read of it.
+template <int N, int FPB, bool DB>
+struct FftGroup {
+    using S = FftShape<N>;
+    static constexpr int T = S::T;
+    static constexpr int STRIDE = (DB ? 2 : 1) * S::SMEM_PAD;  // float2 per group
+    static constexpr int BYTES = FPB * STRIDE * (int)sizeof(float2);  // per block
+    float2* base;
+    int f;
+    int k;
+
+    __device__ __forceinline__ FftGroup(float2* smem_block, int group) : base(smem_block + group * STRIDE), f(group), k(0) {}
+
+    __device__ __forceinline__ void sync() const {
+        if constexpr (T >= 32 && FPB > 1 && FPB <= 15) {
+            asm volatile("bar.sync %0, %1;" ::"r"(f + 1), "n"(T) : "memory");
+        } else {
+            __syncthreads();
+        }
+    }
+
+    // Buffer for the next exchange (waits for the previous readers when single-buffered).
+    __device__ __forceinline__ float2* begin() {
+        float2* p = base;
+        if constexpr (DB) {
+            p += (k & 1) * S::SMEM_PAD;
+        } else {
+            sync();
+        }
+        k++;
+        return p;
+    }
+};
+
 template <int N, bool INV>
 struct BlockFft {
     using S = FftShape<N>;
     static constexpr int T = S::T;
 
-    // Thread j of the FFT, v holds x[j + T q].  s: this FFT's exchange buffer
-    // (S::SMEM float2).  tw: the twiddle table for size N.  qnz: number of leading
-    // q slots that may be non-zero on input (16 = no pruning).
-    // All threads of the block must call this (it contains __syncthreads()).
-    __device__ __forceinline__ static void run(float2 (&v)[16], float2* __restrict__ s, int j,
-                                               const float2* __restrict__ tw, int qnz) {
+    // Thread j of the FFT, v holds x[j + T q].  g: this FFT group's exchange buffers and
+    // barrier.  tw: the twiddle table for size N.  qnz: number of leading q slots that
+    // may be non-zero on input (16 = no pruning).  Every thread of the group must call
+    // this (and, for groups smaller than a warp, every thread of the block).
+    template <class G>
+    __device__ __forceinline__ static void run(float2 (&v)[16], G& g, int j, const float2* __restrict__ tw, int qnz) {
         if constexpr (S::REM > 1) {
             constexpr int R = S::REM;
             constexpr int M = 16 / R;
             first_pass<R, M>(v);
-            __syncthreads();
+            float2* s = g.begin();
 #pragma unroll
             for (int m = 0; m < M; m++) {
                 const int b = j + T * m;
 #pragma unroll
                 for (int r = 0; r < R; r++) s[phys(b * R + r)] = v[m + r * M];
             }
-            __syncthreads();
+            g.sync();
 #pragma unroll
             for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
         }
@@ -370,11 +415,11 @@ struct BlockFft {
             else
                 dft16<INV>(v);
             if (p < S::NP16 - 1) {
-                __syncthreads();
+                float2* s = g.begin();
                 const int base = (j / ns) * 16 * ns + (j & (ns - 1));
 #pragma unroll
                 for (int r = 0; r < 16; r++) s[phys(base + r * ns)] = v[r];
-                __syncthreads();
+                g.sync();
 #pragma unroll
                 for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
             }

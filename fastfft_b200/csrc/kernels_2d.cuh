@@ -95,9 +95,11 @@ r2c_rows_kernel(RowFwdArgs a) {
     using S = FftShape<N>;
     constexpr int T = S::T;
     extern __shared__ float2 smem[];
+    using G = FftGroup<N, FPB, false>;
     const int f = threadIdx.x / T;
     const int j = threadIdx.x - f * T;
-    float2* s = smem + f * S::SMEM;
+    G g(smem, f);
+    float2* s = g.base;
     const int ra = 2 * (blockIdx.x * FPB + f);
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
     const InT* pa = static_cast<const InT*>(a.in[blockIdx.y]) + (long long)ra * a.in_pitch;
@@ -114,7 +116,7 @@ r2c_rows_kernel(RowFwdArgs a) {
         }
         v[q] = make_float2(xa * a.scale, xb * a.scale);
     }
-    BlockFft<N, false>::run(v, s, j, a.tw, leading_slots<T>(a.L, j));
+    BlockFft<N, false>::run(v, g, j, a.tw, leading_slots<T>(a.L, j));
 
     // Split Z = A + iB into the two real-row spectra: A[k] = (Z[k] + conj Z[N-k]) / 2,
     // B[k] = -i (Z[k] - conj Z[N-k]) / 2.
@@ -126,7 +128,7 @@ r2c_rows_kernel(RowFwdArgs a) {
     for (int i = threadIdx.x; i < items; i += blockDim.x) {
         const int ff = i % FPB;
         const int k = i / FPB;
-        const float2* sf = smem + ff * S::SMEM;
+        const float2* sf = smem + ff * G::STRIDE;
         const float2 z1 = sf[phys(k)];
         const float2 z2 = sf[phys((N - k) & (N - 1))];
         const float2 A = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
@@ -173,13 +175,14 @@ cols_kernel(ColArgs a) {
     using S = FftShape<N>;
     constexpr int T = S::T;
     extern __shared__ float2 smem[];
+    using G = FftGroup<N, FPB, true>;
     const int f = threadIdx.x / T;
     const int j = threadIdx.x - f * T;
-    float2* s = smem + f * S::SMEM;
+    G g(smem, f);
     const int col = blockIdx.x * FPB + f;
     const bool valid = col < a.n_cols;
-    const long long g = blockIdx.y;
-    const InC* pin = static_cast<const InC*>(a.in) + g * a.in_batch_stride + (long long)col * a.in_stride;
+    const long long bz = blockIdx.y;
+    const InC* pin = static_cast<const InC*>(a.in) + bz * a.in_batch_stride + (long long)col * a.in_stride;
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
@@ -190,13 +193,13 @@ cols_kernel(ColArgs a) {
     }
     const int qnz = valid ? leading_slots<T>(a.L, j) : 0;
     if constexpr (MODE == COL_INV) {
-        BlockFft<N, true>::run(v, s, j, a.tw, qnz);
+        BlockFft<N, true>::run(v, g, j, a.tw, qnz);
     } else {
-        BlockFft<N, false>::run(v, s, j, a.tw, qnz);
+        BlockFft<N, false>::run(v, g, j, a.tw, qnz);
     }
     if constexpr (MODE == COL_XCORR) {
         if (a.intra_kind != 0) {
-            const ImgC* pimg = static_cast<const ImgC*>(a.img) + g * a.img_batch_stride + (long long)col * a.img_stride;
+            const ImgC* pimg = static_cast<const ImgC*>(a.img) + bz * a.img_batch_stride + (long long)col * a.img_stride;
             const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
 #pragma unroll
             for (int q = 0; q < 16; q++) {
@@ -206,10 +209,10 @@ cols_kernel(ColArgs a) {
                 v[q] = (sc != 1.f) ? cscale(p, sc) : p;
             }
         }
-        BlockFft<N, true>::run(v, s, j, a.tw, 16);
+        BlockFft<N, true>::run(v, g, j, a.tw, 16);
     }
     if (valid) {
-        OutC* pout = static_cast<OutC*>(a.out) + g * a.out_batch_stride + (long long)col * a.out_stride;
+        OutC* pout = static_cast<OutC*>(a.out) + bz * a.out_batch_stride + (long long)col * a.out_stride;
 #pragma unroll
         for (int q = 0; q < 16; q++) {
             const int n = j + T * q;
@@ -244,9 +247,11 @@ c2r_rows_kernel(RowInvArgs a) {
     constexpr int T = S::T;
     constexpr int H = N / 2;
     extern __shared__ float2 smem[];
+    using G = FftGroup<N, FPB, false>;
     const int f = threadIdx.x / T;
     const int j = threadIdx.x - f * T;
-    float2* s = smem + f * S::SMEM;
+    G g(smem, f);
+    float2* s = g.base;
     // Gather rows (2 per FFT) and build Z[k] = A[k] + i B[k] over the full circle
     // from the half spectrum (A, B Hermitian).  The imaginary parts of the k = 0
     // and k = N/2 bins are dropped, as a C2R of a Hermitian spectrum does.
@@ -264,7 +269,7 @@ c2r_rows_kernel(RowInvArgs a) {
         } else if (rr < a.n_rows) {
             A = *p;
         }
-        float2* sf = smem + ff * S::SMEM;
+        float2* sf = smem + ff * G::STRIDE;
         if (k == 0 || k == H) {
             sf[phys(k)] = make_float2(A.x, B.x);
         } else {
@@ -276,7 +281,7 @@ c2r_rows_kernel(RowInvArgs a) {
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
-    BlockFft<N, true>::run(v, s, j, a.tw, 16);
+    BlockFft<N, true>::run(v, g, j, a.tw, 16);
     const int ra = 2 * (blockIdx.x * FPB + f);
     OutT* oa = static_cast<OutT*>(a.out[blockIdx.y]) + (long long)ra * a.out_pitch;
     OutT* ob = oa + a.out_pitch;

@@ -67,6 +67,26 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
     return false;
 }
 
+// Shared-memory loads of the staged image column, kept at their point of use (a plain
+// load could be hoisted above the forward transform, holding 16 more complex values live
+// across it and pushing the kernel past its register budget).
+template <class T> __device__ __forceinline__ float2 lds_cplx(const T* p);
+template <> __device__ __forceinline__ float2 lds_cplx<float2>(const float2* p) {
+    float2 r;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(r.x), "=f"(r.y) : "r"(smem_addr(p)));
+    return r;
+}
+template <> __device__ __forceinline__ float2 lds_cplx<__half2>(const __half2* p) {
+    unsigned int u;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(u) : "r"(smem_addr(p)));
+    return __half22float2(*reinterpret_cast<__half2*>(&u));
+}
+template <> __device__ __forceinline__ float2 lds_cplx<__nv_bfloat162>(const __nv_bfloat162* p) {
+    unsigned int u;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(u) : "r"(smem_addr(p)));
+    return __bfloat1622float2(*reinterpret_cast<__nv_bfloat162*>(&u));
+}
+
 struct XcorrColArgs {
     const float2* t1;          // template g, column c: t1 + g * t1_batch + c * t1_pitch (L valid values)
     long long t1_pitch;
@@ -90,7 +110,7 @@ struct XcorrColArgs {
 template <int N, class ImgC, int FPB>
 struct XcorrSmem {
     static constexpr int kImgBytes = N * (int)sizeof(ImgC);
-    static constexpr int kXchBytes = FPB * FftShape<N>::SMEM * (int)sizeof(float2);
+    static constexpr int kXchBytes = FftGroup<N, FPB, true>::BYTES;
     static __host__ __device__ constexpr int t1_col_elems(int L) { return (L + 1) & ~1; }  // 16-byte multiple
     static __host__ __device__ constexpr int img_off() { return 0; }
     static __host__ __device__ constexpr int xch_off() { return (kImgBytes + 127) & ~127; }
@@ -105,7 +125,11 @@ struct XcorrSmem {
 #define FFB_XCORR_MIN_BLOCKS 2
 #endif
 
-template <int N, class ImgC, int FPB>
+// MUL: apply the conj-multiply intra-op (CONJ_MUL or CONJ_MUL_THEN_SCALE; the scale is
+// 1 for CONJ_MUL, an exact multiplication); without it the kernel is a forward/inverse
+// round trip (NOOP intra-op).  A compile-time choice keeps the transforms free of a
+// run-time branch between them, which costs registers.
+template <int N, class ImgC, int FPB, bool MUL>
 __global__ void __launch_bounds__(FftShape<N>::T * FPB, FFB_XCORR_MIN_BLOCKS)
 xcorr_cols_kernel(XcorrColArgs a) {
     using S = FftShape<N>;
@@ -142,11 +166,14 @@ xcorr_cols_kernel(XcorrColArgs a) {
 
     const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
     const int rounds = (a.n_batch + FPB - 1) / FPB;
-    float2* s = xch + f * S::SMEM;
+    FftGroup<N, FPB, true> grp(xch, f);
 #pragma unroll 1
     for (int it = 0; it < rounds; it++) {
         const int g = it * FPB + f;
         const bool live = g < a.n_batch;
+        // keep the next template's loads from being scheduled into this template's
+        // transforms (that would hold twice the values live and spill)
+        asm volatile("" ::: "memory");
         float2 v[16];
         const float2* src = t1_s + (live ? g : 0) * lcol;
 #pragma unroll
@@ -154,16 +181,15 @@ xcorr_cols_kernel(XcorrColArgs a) {
             const int n = j + T * q;
             v[q] = (live && n < a.L) ? src[n] : make_float2(0.f, 0.f);
         }
-        BlockFft<N, false>::run(v, s, j, a.tw, live ? leading_slots<T>(a.L, j) : 0);
-        if (a.intra_kind != 0) {
+        BlockFft<N, false>::run(v, grp, j, a.tw, live ? leading_slots<T>(a.L, j) : 0);
+        if constexpr (MUL) {
 #pragma unroll
             for (int q = 0; q < 16; q++) {
-                const float2 im = ld_cplx<ImgC>(img_s + j + T * q);
-                const float2 p = conj_mul(v[q], im);
-                v[q] = (sc != 1.f) ? cscale(p, sc) : p;
+                const float2 im = lds_cplx<ImgC>(img_s + j + T * q);
+                v[q] = cscale(conj_mul(v[q], im), sc);
             }
         }
-        BlockFft<N, true>::run(v, s, j, a.tw, 16);
+        BlockFft<N, true>::run(v, grp, j, a.tw, 16);
         if (live) {
             float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
 #pragma unroll

@@ -7,7 +7,7 @@ template <int N, int MODE, class ImgC, class InC = float2>
 static cudaError_t cols_impl(const ColArgs& a, cudaStream_t st) {
     constexpr int FPB = col_fpb<N>();
     constexpr int THREADS = FftShape<N>::T * FPB;
-    const size_t smem = (size_t)FPB * FftShape<N>::SMEM * sizeof(float2);
+    const size_t smem = (size_t)FftGroup<N, FPB, true>::BYTES;
     static std::atomic<unsigned long long> mask{0};
     auto fn = cols_kernel<N, MODE, InC, ImgC, float2, FPB>;
     cudaError_t e = ensure_smem_attr((const void*)fn, smem, &mask);

@@ -7,7 +7,7 @@ template <int N, class InT>
 static cudaError_t r2c_impl(const RowFwdArgs& a, cudaStream_t st) {
     constexpr int FPB = row_fpb<N>();
     constexpr int THREADS = FftShape<N>::T * FPB;
-    const size_t smem = (size_t)FPB * FftShape<N>::SMEM * sizeof(float2);
+    const size_t smem = (size_t)FftGroup<N, FPB, false>::BYTES;
     static std::atomic<unsigned long long> mask{0};
     auto fn = r2c_rows_kernel<N, InT, FPB>;
     cudaError_t e = ensure_smem_attr((const void*)fn, smem, &mask);
@@ -37,7 +37,7 @@ template <int N, class OutT>
 static cudaError_t c2r_impl(const RowInvArgs& a, cudaStream_t st) {
     constexpr int FPB = row_fpb<N>();
     constexpr int THREADS = FftShape<N>::T * FPB;
-    const size_t smem = (size_t)FPB * FftShape<N>::SMEM * sizeof(float2);
+    const size_t smem = (size_t)FftGroup<N, FPB, false>::BYTES;
     static std::atomic<unsigned long long> mask{0};
     auto fn = c2r_rows_kernel<N, OutT, FPB>;
     cudaError_t e = ensure_smem_attr((const void*)fn, smem, &mask);

@@ -16,9 +16,10 @@ static cudaError_t xcorr_v2_impl(const XcorrColArgs& a, cudaStream_t st) {
         if (a.n_batch < 1 || a.n_batch > kMaxBatch || a.n_cols < 1) return cudaErrorInvalidValue;
         const int smem = SM::total(a.L, a.n_batch);
         if (smem > kMaxDynSmem) return cudaErrorInvalidValue;
-        static std::atomic<unsigned long long> mask{0};
-        auto fn = xcorr_cols_kernel<N, ImgC, FPB>;
-        cudaError_t e = ensure_smem_attr((const void*)fn, kMaxDynSmem, &mask);
+        static std::atomic<unsigned long long> mask_mul{0}, mask_nomul{0};
+        const bool mul = a.intra_kind != 0;
+        auto fn = mul ? xcorr_cols_kernel<N, ImgC, FPB, true> : xcorr_cols_kernel<N, ImgC, FPB, false>;
+        cudaError_t e = ensure_smem_attr((const void*)fn, kMaxDynSmem, mul ? &mask_mul : &mask_nomul);
         if (e != cudaSuccess) return e;
         fn<<<a.n_cols, FftShape<N>::T * FPB, smem, st>>>(a);
         return cudaGetLastError();
@@ -43,7 +44,8 @@ size_t xcorr_cols_smem(int n, int img_dtype, int L, int n_batch) {
     const int isz = img_dtype == 3 ? 8 : 4;
     const int fpb = (n / 16) >= 256 ? 1 : 256 / (n / 16);
     const size_t img = ((size_t)n * isz + 127) & ~(size_t)127;
-    const size_t xch = (size_t)fpb * (n + n / 16) * 8;
+    const size_t smem_fft = (size_t)(((n + n / 16) + 15) / 16) * 16 + 4;  // FftShape::SMEM_PAD
+    const size_t xch = (size_t)fpb * 2 * smem_fft * 8;                    // double-buffered groups
     const size_t t1 = (size_t)n_batch * (size_t)((L + 1) & ~1) * 8;
     return ((img + xch + t1 + 15) & ~(size_t)15) + 16;
 }

@@ -1,0 +1,228 @@
+// FastFFT.h -- header-only C++ drop-in for FastFFT::FourierTransformer over the C ABI of
+// libfastfft_b200.so (include/fastfft_capi.h).
+//
+// Mirrors the reference class template (reference include/FastFFT.h:84-219): the same
+// template parameters, method names, argument order and defaults, functor objects
+// (reference include/detail/functors.h:15-80) and error behaviour -- a user error prints
+// the message and calls std::abort(), as MyFFTRunTimeAssert does
+// (reference include/detail/checks_and_debug.h:86-87).  Define FASTFFT_B200_THROW before
+// including this header to get std::runtime_error instead.
+//
+// Differences a caller can see:
+//   - InputType may also be __nv_bfloat16 and OtherImageType __nv_bfloat162;
+//   - the cross-correlation with a forward increase and an inverse decrease (the
+//     reference's "work in progress" abort, FastFFT.cu:673-679) is implemented;
+//   - work goes to cudaStreamPerThread unless SetStream() is called.
+#ifndef FASTFFT_B200_FASTFFT_H
+#define FASTFFT_B200_FASTFFT_H
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <vector_types.h>
+
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "fastfft_capi.h"
+
+namespace FastFFT {
+
+namespace KernelFunction {
+
+// Functor kinds (reference include/detail/functors.h).
+enum IKF_t { NOOP, CONJ_MUL, CONJ_MUL_THEN_SCALE, SCALE };
+
+template <typename T, int N_ARGS, IKF_t U, typename = void>
+struct my_functor {};
+
+template <typename T>
+struct my_functor<T, 0, NOOP> {
+    fastfft_op op() const { return fastfft_op{FASTFFT_OP_NOOP, 1.f}; }
+};
+
+template <typename T>
+struct my_functor<T, 4, CONJ_MUL> {
+    fastfft_op op() const { return fastfft_op{FASTFFT_OP_CONJ_MUL, 1.f}; }
+};
+
+template <typename T>
+struct my_functor<T, 4, CONJ_MUL_THEN_SCALE> {
+    explicit my_functor(const T& scale_factor) : scale_factor(scale_factor) {}
+    fastfft_op op() const { return fastfft_op{FASTFFT_OP_CONJ_MUL_THEN_SCALE, static_cast<float>(scale_factor)}; }
+    const T scale_factor;
+};
+
+template <typename T>
+struct my_functor<T, 2, SCALE> {
+    explicit my_functor(const T& scale_factor) : scale_factor(scale_factor) {}
+    fastfft_op op() const { return fastfft_op{FASTFFT_OP_SCALE, static_cast<float>(scale_factor)}; }
+    const T scale_factor;
+};
+
+}  // namespace KernelFunction
+
+namespace detail {
+
+template <class T>
+constexpr int real_dtype() {
+    if constexpr (std::is_same_v<T, float>) return FASTFFT_DTYPE_F32;
+    else if constexpr (std::is_same_v<T, __half>) return FASTFFT_DTYPE_F16;
+    else if constexpr (std::is_same_v<T, __nv_bfloat16>) return FASTFFT_DTYPE_BF16;
+    else return -1;
+}
+
+template <class T>
+constexpr int complex_dtype() {
+    if constexpr (std::is_same_v<T, float2>) return FASTFFT_DTYPE_C64;
+    else if constexpr (std::is_same_v<T, __half2>) return FASTFFT_DTYPE_C32H;
+    else if constexpr (std::is_same_v<T, __nv_bfloat162>) return FASTFFT_DTYPE_C32BF;
+    else return -1;
+}
+
+template <class Op>
+inline const fastfft_op* op_ptr(const Op& o, fastfft_op& storage) {
+    if constexpr (std::is_same_v<Op, std::nullptr_t>) {
+        return nullptr;
+    } else {
+        storage = o.op();
+        return &storage;
+    }
+}
+
+}  // namespace detail
+
+template <class ComputeBaseType = float, class InputType = float, class OtherImageType = float2, int Rank = 2>
+class FourierTransformer {
+    static_assert(std::is_same_v<ComputeBaseType, float>, "Compute base type must be float");
+    static_assert(Rank == 2 || Rank == 3, "Only 2D and 3D FFTs are supported");
+    static_assert(detail::real_dtype<InputType>() >= 0, "Input type must be float, __half or __nv_bfloat16");
+    static_assert(detail::complex_dtype<OtherImageType>() >= 0,
+                  "OtherImageType must be float2, __half2 or __nv_bfloat162");
+
+  public:
+    FourierTransformer() {
+        check(fastfft_create(&h_, FASTFFT_DTYPE_F32, detail::real_dtype<InputType>(),
+                             detail::complex_dtype<OtherImageType>(), Rank),
+              "FourierTransformer");
+    }
+    ~FourierTransformer() { fastfft_destroy(h_); }
+
+    FourierTransformer(const FourierTransformer&) = delete;
+    FourierTransformer& operator=(const FourierTransformer&) = delete;
+    FourierTransformer(FourierTransformer&&) = delete;
+    FourierTransformer& operator=(FourierTransformer&&) = delete;
+
+    void SetForwardFFTPlan(size_t input_logical_x_dimension, size_t input_logical_y_dimension,
+                           size_t input_logical_z_dimension, size_t output_logical_x_dimension,
+                           size_t output_logical_y_dimension, size_t output_logical_z_dimension,
+                           bool is_padded_output = true) {
+        check(fastfft_set_forward_plan(h_, input_logical_x_dimension, input_logical_y_dimension,
+                                       input_logical_z_dimension, output_logical_x_dimension,
+                                       output_logical_y_dimension, output_logical_z_dimension, is_padded_output),
+              "SetForwardFFTPlan");
+    }
+
+    void SetInverseFFTPlan(size_t input_logical_x_dimension, size_t input_logical_y_dimension,
+                           size_t input_logical_z_dimension, size_t output_logical_x_dimension,
+                           size_t output_logical_y_dimension, size_t output_logical_z_dimension,
+                           bool is_padded_output = true) {
+        check(fastfft_set_inverse_plan(h_, input_logical_x_dimension, input_logical_y_dimension,
+                                       input_logical_z_dimension, output_logical_x_dimension,
+                                       output_logical_y_dimension, output_logical_z_dimension, is_padded_output),
+              "SetInverseFFTPlan");
+    }
+
+    inline void Wait() { check(fastfft_wait(h_), "Wait"); }
+
+    // Extension: run on `stream` instead of cudaStreamPerThread.
+    void SetStream(cudaStream_t stream) { check(fastfft_set_stream(h_, stream), "SetStream"); }
+
+    template <class PreOpType = std::nullptr_t, class IntraOpType = std::nullptr_t>
+    void FwdFFT(InputType* input_ptr, InputType* output_ptr = nullptr, PreOpType pre_op = nullptr,
+                IntraOpType intra_op = nullptr) {
+        fastfft_op a, b;
+        check(fastfft_fwd(h_, input_ptr, output_ptr, detail::op_ptr(pre_op, a), detail::op_ptr(intra_op, b)),
+              "FwdFFT");
+    }
+
+    template <class IntraOpType = std::nullptr_t, class PostOpType = std::nullptr_t>
+    void InvFFT(InputType* input_ptr, InputType* output_ptr = nullptr, IntraOpType intra_op = nullptr,
+                PostOpType post_op = nullptr) {
+        fastfft_op a, b;
+        check(fastfft_inv(h_, input_ptr, output_ptr, detail::op_ptr(intra_op, a), detail::op_ptr(post_op, b)),
+              "InvFFT");
+    }
+
+    template <class PreOpType = std::nullptr_t, class IntraOpType = std::nullptr_t,
+              class PostOpType = std::nullptr_t>
+    void FwdImageInvFFT(InputType* input_ptr, OtherImageType* image_to_search, InputType* output_ptr = nullptr,
+                        PreOpType pre_op = nullptr, IntraOpType intra_op = nullptr, PostOpType post_op = nullptr) {
+        static_assert(!std::is_same_v<IntraOpType, std::nullptr_t>, "FwdImageInvFFT needs an intra-op functor");
+        fastfft_op a, b, c;
+        check(fastfft_fwd_image_inv(h_, input_ptr, image_to_search, output_ptr, detail::op_ptr(pre_op, a),
+                                    detail::op_ptr(intra_op, b), detail::op_ptr(post_op, c)),
+              "FwdImageInvFFT");
+    }
+
+    // Extension: many templates in one call (see fastfft_fwd_image_inv_many).
+    template <class PreOpType = std::nullptr_t, class IntraOpType = std::nullptr_t,
+              class PostOpType = std::nullptr_t>
+    void FwdImageInvFFTMany(int n, InputType* const* inputs, OtherImageType* const* images,
+                            InputType* const* outputs, PreOpType pre_op = nullptr, IntraOpType intra_op = nullptr,
+                            PostOpType post_op = nullptr) {
+        std::vector<const void*> in(inputs, inputs + n), im(images, images + n);
+        std::vector<void*> out;
+        if (outputs) out.assign(outputs, outputs + n);
+        fastfft_op a, b, c;
+        check(fastfft_fwd_image_inv_many(h_, n, in.data(), im.data(), outputs ? out.data() : nullptr,
+                                         detail::op_ptr(pre_op, a), detail::op_ptr(intra_op, b),
+                                         detail::op_ptr(post_op, c)),
+              "FwdImageInvFFTMany");
+    }
+
+    int ReturnInputMemorySize() { return static_cast<int>(ll(fastfft_input_memory_size)); }
+    int ReturnFwdOutputMemorySize() { return static_cast<int>(ll(fastfft_fwd_output_memory_size)); }
+    int ReturnInvOutputMemorySize() { return static_cast<int>(ll(fastfft_inv_output_memory_size)); }
+
+    short4 ReturnFwdInputDimensions() { return dims(fastfft_fwd_input_dims); }
+    short4 ReturnFwdOutputDimensions() { return dims(fastfft_fwd_output_dims); }
+    short4 ReturnInvInputDimensions() { return dims(fastfft_inv_input_dims); }
+    short4 ReturnInvOutputDimensions() { return dims(fastfft_inv_output_dims); }
+
+  private:
+    void check(fastfft_status st, const char* where) {
+        if (st == FASTFFT_OK) return;
+        std::string msg = std::string("FastFFT ") + where + ": " + fastfft_status_string(st) + ": " +
+                          fastfft_last_error(h_);
+#ifdef FASTFFT_B200_THROW
+        throw std::runtime_error(msg);
+#else
+        std::fprintf(stderr, "%s\n", msg.c_str());
+        std::abort();
+#endif
+    }
+
+    long long ll(fastfft_status (*fn)(fastfft_handle, long long*)) {
+        long long v = 0;
+        check(fn(h_, &v), "size query");
+        return v;
+    }
+
+    short4 dims(fastfft_status (*fn)(fastfft_handle, int*)) {
+        int d[4] = {0, 0, 0, 0};
+        check(fn(h_, d), "dimension query");
+        return make_short4((short)d[0], (short)d[1], (short)d[2], (short)d[3]);
+    }
+
+    fastfft_handle h_ = nullptr;
+};
+
+}  // namespace FastFFT
+
+#endif  // FASTFFT_B200_FASTFFT_H

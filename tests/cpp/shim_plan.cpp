@@ -1,0 +1,26 @@
+// Host-only check of the C++ drop-in header: plans and size queries (no GPU needed).
+#define FASTFFT_B200_THROW
+#include <cstdio>
+#include <stdexcept>
+
+#include "FastFFT.h"
+
+int main() {
+    FastFFT::FourierTransformer<float, float, float2, 2> ft;
+    ft.SetForwardFFTPlan(384, 384, 1, 4096, 4096, 1, true);
+    ft.SetInverseFFTPlan(4096, 4096, 1, 1024, 1024, 1, true);
+    short4 o = ft.ReturnFwdOutputDimensions();
+    std::printf("%d %d %d %d %d %d %d %d\n", ft.ReturnInputMemorySize(), ft.ReturnFwdOutputMemorySize(),
+                ft.ReturnInvOutputMemorySize(), (int)o.x, (int)o.y, (int)o.z, (int)o.w,
+                (int)ft.ReturnInvOutputDimensions().w);
+    FastFFT::FourierTransformer<float, __half, __half2, 3> ft3;
+    ft3.SetForwardFFTPlan(64, 64, 64, 256, 256, 256);
+    try {
+        ft3.SetInverseFFTPlan(256, 256, 256, 1024, 1024, 1024);  // > 512 in 3D
+        std::printf("no error\n");
+        return 1;
+    } catch (const std::runtime_error& e) {
+        std::printf("rejected: %s\n", e.what());
+    }
+    return 0;
+}
