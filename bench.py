@@ -70,8 +70,9 @@ def measured_hbm_peak():
 
 
 def ncu_traffic_per_template():
-    """DRAM bytes (read + write) per launch of the fused column kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "xcorr_cols_4096_template384_window1024.md")
+    """DRAM bytes (read + write) per launch of the batched fused column kernel (8 templates),
+    from the committed ncu summary of that kernel."""
+    p = os.path.join(ROOT, "profiles", "xcorr_cols_batched_2048_template384_window1024.md")
     try:
         for line in open(p):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -366,6 +367,9 @@ def run_ours(args, world, rank, local):
                          "kernel": ["r2c_rows", "cols_xcorr", "c2r_rows"][dom],
                          "algorithmic_bytes_per_template": ALG_BYTES_PER_TEMPLATE,
                          "templates_per_launch": n_templates / max(n_calls, 1),
+                         "algorithmic_bytes_per_launch": ALG_BYTES_PER_TEMPLATE * n_templates / max(n_calls, 1),
+                         "traffic_note": "traffic = ncu DRAM bytes per launch of the batched column kernel "
+                                         "(8 templates at 2048^2)",
                          "pass_us_per_template": per_pass_us,
                          "pipeline_frac": ALG_BYTES_PER_TEMPLATE / (ms * 1e-3 / (args.steps * B)) / 1e9 / peak},
             "cpu_baseline": cpu,

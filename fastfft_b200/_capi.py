@@ -56,6 +56,7 @@ SIGNATURES = {
     "fastfft_set_inverse_plan": (_st, [Handle, _sz, _sz, _sz, _sz, _sz, _sz, ctypes.c_int]),
     "fastfft_set_stream": (_st, [Handle, _vp]),
     "fastfft_set_output_dtype": (_st, [Handle, ctypes.c_int]),
+    "fastfft_set_inverse_output_origin": (_st, [Handle, _sz, _sz, _sz]),
     "fastfft_fwd": (_st, [Handle, _vp, _vp, _op, _op]),
     "fastfft_inv": (_st, [Handle, _vp, _vp, _op, _op]),
     "fastfft_fwd_image_inv": (_st, [Handle, _vp, _vp, _vp, _op, _op, _op]),

@@ -6,6 +6,11 @@
 //   2D FwdFFT          r2c_rows (N_x, L_y rows)  -> cols FWD (N_y)
 //   2D InvFFT          cols INV (N_y, keep W_y)  -> c2r_rows (N_x, keep W_x)
 //   2D FwdImageInvFFT  r2c_rows -> cols XCORR (fwd, conj-mul, inv, keep W_y) -> c2r_rows
+//   3D FwdFFT          r2c_rows (x) -> cols FWD (z, transposed store) -> cols FWD (y)
+//   3D InvFFT          cols INV (y, transposed) -> cols INV (z, transposed) -> c2r_rows (x)
+//   3D FwdImageInvFFT  r2c_rows -> cols FWD (z) -> cols XCORR (y) -> cols INV (z) -> c2r_rows
+// Intermediate layouts: forward [kx][y][z] then [kz][kx][y]; spectrum [kz][kx][ky];
+// inverse [kx][y'][kz] then [kx][z'][y'] (primes: retained window coordinates).
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -104,6 +109,8 @@ fastfft_status validate(fastfft_plan_s* h) {
     if (!in_range(nx) || !in_range(ny) || (dim == 3 && !in_range(nz)))
         return fail(h, FASTFFT_ERR_UNSUPPORTED, "transform sizes must be in [16, 8192]");
     if (!in_range(ii.x) || !in_range(ii.y)) return fail(h, FASTFFT_ERR_UNSUPPORTED, "transform sizes must be in [16, 8192]");
+    if (h->org_x + io.x > ii.x || h->org_y + io.y > ii.y || h->org_z + io.z > ii.z)
+        return fail(h, FASTFFT_ERR_INVALID_DIMS, "inverse output window exceeds the transform (origin + size > N)");
     h->validated = true;
     return FASTFFT_OK;
 }
@@ -119,16 +126,31 @@ long long pow2_at_least(long long v) {
 
 void size_buffers(fastfft_plan_s* h) {
     const long long nx_f = std::max(h->fwd_in.x, h->fwd_out.x);
-    h->pitch_a = round_up(h->fwd_in.y, 4);
     const long long kx_f = nx_f / 2 + 1;
+    const long long kx_i = h->inv_in.x / 2 + 1;
+    if (h->rank == 3) {
+        // A: forward [kx][y][z] (pitch round_up(Ly*Lz, 4)) / inverse [kx][y'][kz]
+        // B: forward [kz][kx][y] / inverse [kx][z'][y'] (pitch round_up(Wz*Wy, 4))
+        h->pitch_a = round_up(h->fwd_in.y * h->fwd_in.z, 4);
+        h->pitch_b = round_up(h->inv_out.y * h->inv_out.z, 4);
+        const long long nz_f = std::max(h->fwd_in.z, h->fwd_out.z);
+        const long long a = std::max(kx_f * h->pitch_a, kx_i * h->inv_out.y * h->inv_in.z);
+        const long long b = std::max(nz_f * h->fwd_out.w * h->fwd_in.y, kx_i * h->pitch_b);
+        h->bytes_a = round_up(a * 8, 256);
+        h->bytes_b = round_up(b * 8, 256);
+        h->red_ok = false;
+        h->bytes_c = 0;
+        return;
+    }
+    h->pitch_a = round_up(h->fwd_in.y, 4);
     h->bytes_a = round_up(kx_f * h->pitch_a * 8, 256);
     h->pitch_b = round_up(h->inv_out.y, 4);
-    const long long kx_i = h->inv_in.x / 2 + 1;
     h->bytes_b = round_up(kx_i * h->pitch_b * 8, 256);
     // reduced-size correlation
     h->red_ok = false;
     h->bytes_c = 0;
-    if (h->rank == 2 && h->fwd_change != SizeChange::Decrease && h->inv_change == SizeChange::Decrease) {
+    const bool origin0 = h->org_x == 0 && h->org_y == 0 && h->org_z == 0;
+    if (origin0 && h->fwd_change != SizeChange::Decrease && h->inv_change == SizeChange::Decrease) {
         const long long nx = h->fwd_out.x, ny = h->fwd_out.y;
         const long long mx = std::min(nx, std::max<long long>(ffb::kMinN, pow2_at_least(h->fwd_in.x + h->inv_out.x - 1)));
         const long long my = std::min(ny, std::max<long long>(ffb::kMinN, pow2_at_least(h->fwd_in.y + h->inv_out.y - 1)));
@@ -200,7 +222,6 @@ fastfft_status prepare_call(fastfft_plan_s* h) {
         st = allocate(h);
         if (st != FASTFFT_OK) return st;
     }
-    if (h->rank != 2) return fail(h, FASTFFT_ERR_UNSUPPORTED, "3D transforms are not available in this build");
     return FASTFFT_OK;
 }
 
@@ -229,52 +250,213 @@ void prof_end_call(fastfft_plan_s* h) {
     h->prof_mark = 0;
 }
 
-// Row pass of the forward transform into region A.
-fastfft_status run_fwd_rows(fastfft_plan_s* h, const void* in, float pre_scale, int kmax) {
-    const int nx = (int)std::max(h->fwd_in.x, h->fwd_out.x);
+// ---------------------------------------------------------------------------
+// Stage helpers: one kernel launch each, counted and marked for profiling.
+// ---------------------------------------------------------------------------
+fastfft_status stage_r2c(fastfft_plan_s* h, int n, int in_dtype, const void* in, long long in_pitch, int n_rows,
+                         int rows_y, int rows_z, int L, float2* out, long long out_pitch, int kmax, float scale) {
     const float2* tw = nullptr;
-    cudaError_t e = twiddles_for(nx, &tw);
+    cudaError_t e = twiddles_for(n, &tw);
     if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     RowFwdArgs a;
     std::memset(&a, 0, sizeof(a));
     a.in[0] = in;
     a.n_batch = 1;
-    a.in_pitch = 2LL * h->fwd_in.w;
-    a.n_rows = (int)h->fwd_in.y;
-    a.L = (int)h->fwd_in.x;
-    a.out = region_a(h);
-    a.out_pitch = h->pitch_a;
+    a.in_pitch = in_pitch;
+    a.n_rows = n_rows;
+    a.rows_y = rows_y;
+    a.rows_z = rows_z;
+    a.L = L;
+    a.out = out;
+    a.out_pitch = out_pitch;
     a.kmax = kmax;
-    a.scale = pre_scale;
+    a.scale = scale;
     a.tw = tw;
-    e = launch_r2c_rows(nx, h->input_dtype, a, h->stream);
+    e = launch_r2c_rows(n, in_dtype, a, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "r2c row pass");
     h->launches++;
     prof_mark(h);
     return FASTFFT_OK;
 }
 
-fastfft_status run_inv_rows(fastfft_plan_s* h, void* out, float post_scale) {
-    const int nx = (int)h->inv_in.x;
+fastfft_status stage_c2r(fastfft_plan_s* h, int n, const float2* in, long long in_pitch, int n_rows, void* out,
+                         long long out_pitch, int W, int X0, float scale) {
     const float2* tw = nullptr;
-    cudaError_t e = twiddles_for(nx, &tw);
+    cudaError_t e = twiddles_for(n, &tw);
     if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     RowInvArgs a;
     std::memset(&a, 0, sizeof(a));
     a.n_batch = 1;
-    a.in = region_b(h);
-    a.in_pitch = h->pitch_b;
-    a.n_rows = (int)h->inv_out.y;
+    a.in = in;
+    a.in_pitch = in_pitch;
+    a.n_rows = n_rows;
     a.out[0] = out;
-    a.out_pitch = 2LL * h->inv_out.w;
-    a.W = (int)h->inv_out.x;
-    a.scale = post_scale;
+    a.out_pitch = out_pitch;
+    a.W = W;
+    a.X0 = X0;
+    a.scale = scale;
     a.tw = tw;
-    e = launch_c2r_rows(nx, h->output_dtype, a, h->stream);
+    e = launch_c2r_rows(n, h->output_dtype, a, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "c2r row pass");
     h->launches++;
     prof_mark(h);
     return FASTFFT_OK;
+}
+
+// Column arguments with the plain layout (column c at c * in_stride / c * out_stride).
+ColArgs col_args(const void* in, long long in_stride, int L, void* out, long long out_stride, int W, int n_cols) {
+    ColArgs c;
+    std::memset(&c, 0, sizeof(c));
+    c.in = in;
+    c.in_stride = in_stride;
+    c.L = L;
+    c.out = out;
+    c.out_stride = out_stride;
+    c.W = W;
+    c.n_cols = n_cols;
+    c.in_scale = 1.f;
+    c.out_scale = 1.f;
+    c.intra_scale = 1.f;
+    c.n_batch = 1;
+    return c;
+}
+
+enum StageMode { ST_FWD, ST_INV, ST_XCORR };
+
+fastfft_status stage_cols(fastfft_plan_s* h, int n, StageMode mode, int dtype, ColArgs& c) {
+    const float2* tw = nullptr;
+    cudaError_t e = twiddles_for(n, &tw);
+    if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
+    c.tw = tw;
+    if (mode == ST_FWD)
+        e = launch_cols_fwd(n, c, h->stream);
+    else if (mode == ST_INV)
+        e = launch_cols_inv(n, dtype, c, h->stream);
+    else
+        e = launch_cols_xcorr(n, dtype, c, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, mode == ST_XCORR ? "cross-correlation column pass" : "column pass");
+    h->launches++;
+    prof_mark(h);
+    return FASTFFT_OK;
+}
+
+#define FFB_TRY(x)                               \
+    do {                                         \
+        fastfft_status st_ = (x);                \
+        if (st_ != FASTFFT_OK) return st_;       \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Transform sequences
+// ---------------------------------------------------------------------------
+fastfft_status seq_fwd(fastfft_plan_s* h, const void* in, void* out, float pre_scale) {
+    const Dims &fi = h->fwd_in, &fo = h->fwd_out;
+    const int nx = (int)std::max(fi.x, fo.x), ny = (int)std::max(fi.y, fo.y), nz = (int)std::max(fi.z, fo.z);
+    const int kmax = (int)fo.w;
+    if (h->rank == 2) {
+        FFB_TRY(stage_r2c(h, nx, h->input_dtype, in, 2LL * fi.w, (int)fi.y, (int)fi.y, 1, (int)fi.x, region_a(h),
+                          h->pitch_a, kmax, pre_scale));
+        ColArgs c = col_args(region_a(h), h->pitch_a, (int)fi.y, out, fo.y, (int)fo.y, kmax);
+        return stage_cols(h, ny, ST_FWD, FASTFFT_DTYPE_C64, c);
+    }
+    const long long ly = fi.y, lz = fi.z;
+    // x: rows (y, z) -> A[kx][y][z]
+    FFB_TRY(stage_r2c(h, nx, h->input_dtype, in, 2LL * fi.w, (int)(ly * lz), (int)ly, (int)lz, (int)fi.x, region_a(h),
+                      h->pitch_a, kmax, pre_scale));
+    // z: columns (kx, y) -> B[kz][kx][y]
+    ColArgs cz = col_args(region_a(h), h->pitch_a, (int)lz, region_b(h), 1, (int)fo.z, (int)(kmax * ly));
+    cz.in_div = (int)ly;
+    cz.in_stride2 = lz;
+    cz.out_elem_stride = kmax * ly;
+    FFB_TRY(stage_cols(h, nz, ST_FWD, FASTFFT_DTYPE_C64, cz));
+    // y: columns (kz, kx) -> spectrum [kz][kx][ky]
+    ColArgs cy = col_args(region_b(h), ly, (int)ly, out, fo.y, (int)fo.y, (int)(fo.z * kmax));
+    return stage_cols(h, ny, ST_FWD, FASTFFT_DTYPE_C64, cy);
+}
+
+// Inverse from a complex spectrum `in` (dtype in_dtype) of the inverse-input size.
+fastfft_status seq_inv(fastfft_plan_s* h, const void* in, int in_dtype, void* out, float post_scale) {
+    const Dims &ii = h->inv_in, &io = h->inv_out;
+    const int nx = (int)ii.x, ny = (int)ii.y, nz = (int)ii.z;
+    const int kw = nx / 2 + 1;
+    if (h->rank == 2) {
+        ColArgs c = col_args(in, ny, ny, region_b(h), h->pitch_b, (int)io.y, kw);
+        c.W0 = (int)h->org_y;
+        FFB_TRY(stage_cols(h, ny, ST_INV, in_dtype, c));
+        return stage_c2r(h, nx, region_b(h), h->pitch_b, (int)io.y, out, 2LL * io.w, (int)io.x, (int)h->org_x,
+                         post_scale);
+    }
+    const long long wy = io.y, wz = io.z;
+    // y: columns c = kx * Nz + kz -> A[kx][y'][kz]
+    ColArgs cy = col_args(in, ny, ny, region_a(h), wy * nz, (int)wy, (int)(kw * nz));
+    cy.in_div = nz;
+    cy.in_stride2 = (long long)kw * ny;
+    cy.out_div = nz;
+    cy.out_stride2 = 1;
+    cy.out_elem_stride = nz;
+    cy.W0 = (int)h->org_y;
+    FFB_TRY(stage_cols(h, ny, ST_INV, in_dtype, cy));
+    // z: columns c = kx * Wy + y' -> B[kx][z'][y']
+    ColArgs cz = col_args(region_a(h), nz, nz, region_b(h), h->pitch_b, (int)wz, (int)(kw * wy));
+    cz.out_div = (int)wy;
+    cz.out_stride2 = 1;
+    cz.out_elem_stride = wy;
+    cz.W0 = (int)h->org_z;
+    FFB_TRY(stage_cols(h, nz, ST_INV, FASTFFT_DTYPE_C64, cz));
+    // x: rows r = z' * Wy + y'
+    return stage_c2r(h, nx, region_b(h), h->pitch_b, (int)(wz * wy), out, 2LL * io.w, (int)io.x, (int)h->org_x,
+                     post_scale);
+}
+
+// Size-N fused correlation of one template (forward increase or no change).
+fastfft_status seq_xcorr(fastfft_plan_s* h, const void* in, const void* img, void* out, float pre_scale,
+                         const fastfft_op* intra_op, float post_scale) {
+    const Dims &fi = h->fwd_in, &fo = h->fwd_out, &io = h->inv_out;
+    const int nx = (int)fo.x, ny = (int)fo.y, nz = (int)fo.z;
+    const int kw = nx / 2 + 1;
+    const int ikind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
+    const float iscale = intra_op ? intra_op->scale : 1.f;
+    if (h->rank == 2) {
+        FFB_TRY(stage_r2c(h, nx, h->input_dtype, in, 2LL * fi.w, (int)fi.y, (int)fi.y, 1, (int)fi.x, region_a(h),
+                          h->pitch_a, kw, pre_scale));
+        ColArgs c = col_args(region_a(h), h->pitch_a, (int)fi.y, region_b(h), h->pitch_b, (int)io.y, kw);
+        c.img = img;
+        c.img_stride = ny;
+        c.intra_kind = ikind;
+        c.intra_scale = iscale;
+        c.W0 = (int)h->org_y;
+        FFB_TRY(stage_cols(h, ny, ST_XCORR, h->image_dtype, c));
+        return stage_c2r(h, nx, region_b(h), h->pitch_b, (int)io.y, out, 2LL * io.w, (int)io.x, (int)h->org_x,
+                         post_scale);
+    }
+    const long long ly = fi.y, lz = fi.z, wy = io.y, wz = io.z;
+    FFB_TRY(stage_r2c(h, nx, h->input_dtype, in, 2LL * fi.w, (int)(ly * lz), (int)ly, (int)lz, (int)fi.x, region_a(h),
+                      h->pitch_a, kw, pre_scale));
+    ColArgs cz = col_args(region_a(h), h->pitch_a, (int)lz, region_b(h), 1, nz, (int)(kw * ly));
+    cz.in_div = (int)ly;
+    cz.in_stride2 = lz;
+    cz.out_elem_stride = (long long)kw * ly;
+    FFB_TRY(stage_cols(h, nz, ST_FWD, FASTFFT_DTYPE_C64, cz));
+    // y: columns c = kz * kw + kx (B layout); conj-multiply against image column c; inverse;
+    // keep y' -> A[kx][y'][kz]
+    ColArgs cy = col_args(region_b(h), ly, (int)ly, region_a(h), 1, (int)wy, nz * kw);
+    cy.img = img;
+    cy.img_stride = ny;
+    cy.intra_kind = ikind;
+    cy.intra_scale = iscale;
+    cy.out_div = kw;
+    cy.out_stride2 = wy * nz;
+    cy.out_elem_stride = nz;
+    cy.W0 = (int)h->org_y;
+    FFB_TRY(stage_cols(h, ny, ST_XCORR, h->image_dtype, cy));
+    ColArgs ci = col_args(region_a(h), nz, nz, region_b(h), h->pitch_b, (int)wz, (int)(kw * wy));
+    ci.out_div = (int)wy;
+    ci.out_stride2 = 1;
+    ci.out_elem_stride = wy;
+    ci.W0 = (int)h->org_z;
+    FFB_TRY(stage_cols(h, nz, ST_INV, FASTFFT_DTYPE_C64, ci));
+    return stage_c2r(h, nx, region_b(h), h->pitch_b, (int)(wz * wy), out, 2LL * io.w, (int)io.x, (int)h->org_x,
+                     post_scale);
 }
 
 }  // namespace
@@ -375,6 +557,28 @@ fastfft_status fastfft_set_stream(fastfft_handle h, void* cuda_stream) {
     return FASTFFT_OK;
 }
 
+fastfft_status fastfft_set_inverse_output_origin(fastfft_handle h, size_t ox, size_t oy, size_t oz) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (ox >= (1u << 15) || oy >= (1u << 15) || oz >= (1u << 15))
+        return fail(h, FASTFFT_ERR_INVALID_DIMS, "origin out of range");
+    h->org_x = (long long)ox;
+    h->org_y = (long long)oy;
+    h->org_z = (long long)oz;
+    h->validated = false;
+    if (h->fwd_set && h->inv_set) {
+        fastfft_status st = validate(h);
+        if (st != FASTFFT_OK) return st;
+        const size_t before = h->buffer_bytes;
+        size_buffers(h);
+        if (h->buffer && (size_t)(h->bytes_a + h->bytes_b + h->bytes_c) + 256 > before) {
+            cudaFree(h->buffer);
+            h->buffer = nullptr;
+            h->buffer_bytes = 0;
+        }
+    }
+    return FASTFFT_OK;
+}
+
 fastfft_status fastfft_set_output_dtype(fastfft_handle h, int dtype) {
     if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
     if (!real_dtype(dtype)) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "output dtype must be real (f32, f16, bf16)");
@@ -392,34 +596,10 @@ fastfft_status fastfft_fwd(fastfft_handle h, const void* input, void* output, co
     fastfft_status st = prepare_call(h);
     if (st != FASTFFT_OK) return st;
     void* out = output ? output : const_cast<void*>(input);
-    const int kmax = (int)h->fwd_out.w;
     prof_begin_call(h);
-    st = run_fwd_rows(h, input, scale_of(pre_op), kmax);
-    if (st != FASTFFT_OK) return st;
-    const int ny = (int)std::max(h->fwd_in.y, h->fwd_out.y);
-    const float2* tw = nullptr;
-    cudaError_t e = twiddles_for(ny, &tw);
-    if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
-    ColArgs c;
-    std::memset(&c, 0, sizeof(c));
-    c.in = region_a(h);
-    c.in_stride = h->pitch_a;
-    c.L = (int)h->fwd_in.y;
-    c.out = out;
-    c.out_stride = h->fwd_out.y;
-    c.W = (int)h->fwd_out.y;
-    c.n_cols = kmax;
-    c.in_scale = 1.f;
-    c.out_scale = 1.f;
-    c.intra_scale = 1.f;
-    c.tw = tw;
-    c.n_batch = 1;
-    e = launch_cols_fwd(ny, c, h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "forward column pass");
-    h->launches++;
-    prof_mark(h);
+    st = seq_fwd(h, input, out, scale_of(pre_op));
     prof_end_call(h);
-    return FASTFFT_OK;
+    return st;
 }
 
 fastfft_status fastfft_inv(fastfft_handle h, const void* input, void* output, const fastfft_op* intra_op,
@@ -434,30 +614,8 @@ fastfft_status fastfft_inv(fastfft_handle h, const void* input, void* output, co
     if (h->inv_change == SizeChange::Increase)
         return fail(h, FASTFFT_ERR_UNSUPPORTED, "inverse size increase is not supported");
     void* out = output ? output : const_cast<void*>(input);
-    const int ny = (int)h->inv_in.y;
     prof_begin_call(h);
-    const float2* tw = nullptr;
-    cudaError_t e = twiddles_for(ny, &tw);
-    if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
-    ColArgs c;
-    std::memset(&c, 0, sizeof(c));
-    c.in = input;
-    c.in_stride = h->inv_in.y;
-    c.L = (int)h->inv_in.y;
-    c.out = region_b(h);
-    c.out_stride = h->pitch_b;
-    c.W = (int)h->inv_out.y;
-    c.n_cols = (int)h->inv_in.w;
-    c.in_scale = 1.f;
-    c.out_scale = 1.f;
-    c.intra_scale = 1.f;
-    c.tw = tw;
-    c.n_batch = 1;
-    e = launch_cols_inv(ny, FASTFFT_DTYPE_C64, c, h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "inverse column pass");
-    h->launches++;
-    prof_mark(h);
-    st = run_inv_rows(h, out, scale_of(post_op));
+    st = seq_inv(h, input, FASTFFT_DTYPE_C64, out, scale_of(post_op));
     prof_end_call(h);
     return st;
 }
@@ -479,36 +637,8 @@ static fastfft_status xcorr_checks(fastfft_handle h, const fastfft_op* pre_op, c
 
 static fastfft_status xcorr_one(fastfft_handle h, const void* input, const void* image_spectrum, void* out,
                                 const fastfft_op* pre_op, const fastfft_op* intra_op, const fastfft_op* post_op) {
-    const int nx = (int)h->fwd_out.x;
     prof_begin_call(h);
-    fastfft_status st = run_fwd_rows(h, input, scale_of(pre_op), nx / 2 + 1);
-    if (st != FASTFFT_OK) return st;
-    const int ny = (int)h->fwd_out.y;
-    const float2* tw = nullptr;
-    cudaError_t e = twiddles_for(ny, &tw);
-    if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
-    ColArgs c;
-    std::memset(&c, 0, sizeof(c));
-    c.in = region_a(h);
-    c.in_stride = h->pitch_a;
-    c.L = (int)h->fwd_in.y;
-    c.img = image_spectrum;
-    c.img_stride = ny;
-    c.out = region_b(h);
-    c.out_stride = h->pitch_b;
-    c.W = (int)h->inv_out.y;
-    c.n_cols = nx / 2 + 1;
-    c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
-    c.intra_scale = intra_op ? intra_op->scale : 1.f;
-    c.in_scale = 1.f;
-    c.out_scale = 1.f;
-    c.tw = tw;
-    c.n_batch = 1;
-    e = launch_cols_xcorr(ny, h->image_dtype, c, h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cross-correlation column pass");
-    h->launches++;
-    prof_mark(h);
-    st = run_inv_rows(h, out, scale_of(post_op));
+    fastfft_status st = seq_xcorr(h, input, image_spectrum, out, scale_of(pre_op), intra_op, scale_of(post_op));
     prof_end_call(h);
     return st;
 }
@@ -524,42 +654,21 @@ static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spec
     float* crop = reinterpret_cast<float*>(c + h->off_c_real);
     float2* spec = reinterpret_cast<float2*>(c + h->off_c_spec);
     const long long crop_pitch = 2LL * (mx / 2 + 1);
-    const float2* tw = nullptr;
-    cudaError_t e;
-    // 1. inverse along y, keep y < My: stage[kx][y]
-    if ((e = twiddles_for(ny, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
-    ColArgs c1;
-    std::memset(&c1, 0, sizeof(c1));
-    c1.in = image_spectrum; c1.in_stride = ny; c1.L = ny;
-    c1.out = stage; c1.out_stride = my; c1.W = my; c1.n_cols = nx / 2 + 1;
-    c1.in_scale = 1.f; c1.out_scale = 1.f; c1.intra_scale = 1.f; c1.tw = tw; c1.n_batch = 1;
-    if ((e = launch_cols_inv(ny, h->image_dtype, c1, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (inverse columns)");
-    // 2. C2R along x, keep x < Mx: crop[y][x]
-    if ((e = twiddles_for(nx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
-    RowInvArgs r2;
-    std::memset(&r2, 0, sizeof(r2));
-    r2.n_batch = 1;
-    r2.in = stage; r2.in_pitch = my; r2.n_rows = my; r2.out[0] = crop; r2.out_pitch = crop_pitch; r2.W = mx;
-    r2.scale = 1.f; r2.tw = tw;
-    if ((e = launch_c2r_rows(nx, FASTFFT_DTYPE_F32, r2, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (C2R rows)");
+    const int saved_out = h->output_dtype;
+    h->output_dtype = FASTFFT_DTYPE_F32;  // the cropped image is an internal FP32 array
+    // 1. inverse along y keeping y < My: stage[kx][y]
+    ColArgs c1 = col_args(image_spectrum, ny, ny, stage, my, my, nx / 2 + 1);
+    fastfft_status st = stage_cols(h, ny, ST_INV, h->image_dtype, c1);
+    // 2. C2R along x keeping x < Mx: crop[y][x]
+    if (st == FASTFFT_OK) st = stage_c2r(h, nx, stage, my, my, crop, crop_pitch, mx, 0, 1.f);
+    h->output_dtype = saved_out;
+    if (st != FASTFFT_OK) return st;
     // 3. R2C along x at size Mx: stage[kx][y]
-    if ((e = twiddles_for(mx, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
-    RowFwdArgs r3;
-    std::memset(&r3, 0, sizeof(r3));
-    r3.n_batch = 1;
-    r3.in[0] = crop; r3.in_pitch = crop_pitch; r3.n_rows = my; r3.L = mx; r3.out = stage; r3.out_pitch = my;
-    r3.kmax = mx / 2 + 1; r3.scale = 1.f; r3.tw = tw;
-    if ((e = launch_r2c_rows(mx, FASTFFT_DTYPE_F32, r3, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (R2C rows)");
-    // 4. forward along y at size My, scaled: spec[kx][ky]
-    if ((e = twiddles_for(my, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
-    ColArgs c4;
-    std::memset(&c4, 0, sizeof(c4));
-    c4.in = stage; c4.in_stride = my; c4.L = my;
-    c4.out = spec; c4.out_stride = my; c4.W = my; c4.n_cols = mx / 2 + 1;
-    c4.in_scale = 1.f; c4.out_scale = 1.f / ((float)mx * (float)my); c4.intra_scale = 1.f; c4.tw = tw; c4.n_batch = 1;
-    if ((e = launch_cols_fwd(my, c4, h->stream)) != cudaSuccess) return cuda_fail(h, e, "image prep (forward columns)");
-    h->launches += 4;
-    return FASTFFT_OK;
+    FFB_TRY(stage_r2c(h, mx, FASTFFT_DTYPE_F32, crop, crop_pitch, my, my, 1, mx, stage, my, mx / 2 + 1, 1.f));
+    // 4. forward along y at size My, scaled by 1/(Mx My): spec[kx][ky]
+    ColArgs c4 = col_args(stage, my, my, spec, my, my, mx / 2 + 1);
+    c4.out_scale = 1.f / ((float)mx * (float)my);
+    return stage_cols(h, my, ST_FWD, FASTFFT_DTYPE_C64, c4);
 }
 
 // Up to kMaxBatch templates through the reduced-size correlation against the prepared

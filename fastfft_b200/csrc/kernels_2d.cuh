@@ -87,7 +87,16 @@ struct RowFwdArgs {
     float scale;           // pre-op SCALE (1 = NOOP)
     const float2* tw;      // twiddle table of size N
     int n_batch;           // templates in this launch (grid.y)
+    // 3D: flat row r = y * rows_z + z reads input row z * rows_y + y, so that the output
+    // [kx][y][z] has z contiguous.  rows_z <= 1: row r reads input row r.
+    int rows_y;
+    int rows_z;
 };
+
+__device__ __forceinline__ long long input_row(int r, int rows_y, int rows_z) {
+    if (rows_z <= 1) return r;
+    return (long long)(r % rows_z) * rows_y + r / rows_z;
+}
 
 template <int N, class InT, int FPB>
 __global__ void __launch_bounds__(FftShape<N>::T * FPB)
@@ -102,9 +111,10 @@ r2c_rows_kernel(RowFwdArgs a) {
     float2* s = g.base;
     const int ra = 2 * (blockIdx.x * FPB + f);
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
-    const InT* pa = static_cast<const InT*>(a.in[blockIdx.y]) + (long long)ra * a.in_pitch;
+    const InT* in_g = static_cast<const InT*>(a.in[blockIdx.y]);
+    const InT* pa = in_g + input_row(ra, a.rows_y, a.rows_z) * a.in_pitch;
+    const InT* pb = in_g + input_row(ra + 1, a.rows_y, a.rows_z) * a.in_pitch;
     float2* const out_g = a.out + (long long)blockIdx.y * a.out_batch_stride;
-    const InT* pb = pa + a.in_pitch;
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
@@ -167,6 +177,16 @@ struct ColArgs {
     float out_scale;
     const float2* tw;
     int n_batch;             // batch entries in this launch (grid.y)
+    // General addressing (3D passes); zero values select the plain 2D layout above.
+    //   input  column c: (c / in_div) * in_stride + (c % in_div) * in_stride2
+    //   output column c, element n in [W0, W0 + W):
+    //          (c / out_div) * out_stride + (c % out_div) * out_stride2 + (n - W0) * out_elem_stride
+    int in_div;
+    long long in_stride2;
+    int out_div;
+    long long out_stride2;
+    long long out_elem_stride;
+    int W0;
 };
 
 template <int N, int MODE, class InC, class ImgC, class OutC, int FPB>
@@ -182,7 +202,9 @@ cols_kernel(ColArgs a) {
     const int col = blockIdx.x * FPB + f;
     const bool valid = col < a.n_cols;
     const long long bz = blockIdx.y;
-    const InC* pin = static_cast<const InC*>(a.in) + bz * a.in_batch_stride + (long long)col * a.in_stride;
+    const int in_div = a.in_div > 0 ? a.in_div : 1;
+    const InC* pin = static_cast<const InC*>(a.in) + bz * a.in_batch_stride + (long long)(col / in_div) * a.in_stride +
+                     (long long)(col % in_div) * a.in_stride2;
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
@@ -212,13 +234,16 @@ cols_kernel(ColArgs a) {
         BlockFft<N, true>::run(v, g, j, a.tw, 16);
     }
     if (valid) {
-        OutC* pout = static_cast<OutC*>(a.out) + bz * a.out_batch_stride + (long long)col * a.out_stride;
+        const int out_div = a.out_div > 0 ? a.out_div : 1;
+        const long long es = a.out_elem_stride > 0 ? a.out_elem_stride : 1;
+        OutC* pout = static_cast<OutC*>(a.out) + bz * a.out_batch_stride + (long long)(col / out_div) * a.out_stride +
+                     (long long)(col % out_div) * a.out_stride2;
 #pragma unroll
         for (int q = 0; q < 16; q++) {
-            const int n = j + T * q;
-            if (n < a.W) {
+            const int n = j + T * q - a.W0;
+            if (n >= 0 && n < a.W) {
                 float2 x = (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q];
-                pout[n] = x;
+                pout[n * es] = x;
             }
         }
     }
@@ -234,10 +259,11 @@ struct RowInvArgs {
     int n_rows;
     void* out[kMaxBatch];  // real rows of batch entry g: row r at out[g] + r * out_pitch (elements)
     long long out_pitch;
-    int W;                 // x outputs kept per row
+    int W;                 // x outputs kept per row: x in [X0, X0 + W)
     float scale;           // post-op SCALE (1 = NOOP)
     const float2* tw;
     int n_batch;           // batch entries in this launch (grid.y)
+    int X0;
 };
 
 template <int N, class OutT, int FPB>
@@ -288,8 +314,8 @@ c2r_rows_kernel(RowInvArgs a) {
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
 #pragma unroll
     for (int q = 0; q < 16; q++) {
-        const int n = j + T * q;
-        if (n < a.W) {
+        const int n = j + T * q - a.X0;
+        if (n >= 0 && n < a.W) {
             if (has_a) st_real<OutT>(oa + n, v[q].x * a.scale);
             if (has_b) st_real<OutT>(ob + n, v[q].y * a.scale);
         }

@@ -30,6 +30,9 @@ struct fastfft_plan_s {
     bool fwd_set = false, inv_set = false, validated = false;
     ffb::SizeChange fwd_change = ffb::SizeChange::NoChange;
     ffb::SizeChange inv_change = ffb::SizeChange::NoChange;
+    // first retained output per axis of an inverse size decrease (the reference keeps
+    // the window at the origin; fastfft_set_inverse_output_origin moves it)
+    long long org_x = 0, org_y = 0, org_z = 0;
 
     // ReturnInputMemorySize / ReturnFwdOutputMemorySize / ReturnInvOutputMemorySize and
     // compute_memory_wanted_ (element counts, include/FastFFT.h:194-204, :363-404)

@@ -114,6 +114,10 @@ class FourierTransformer:
         self._stream = stream if stream is not None else 0
         self._check(self._lib.fastfft_set_stream(self._h, ctypes.c_void_p(raw) if raw else None))
 
+    def SetInverseOutputOrigin(self, ox, oy, oz=0):
+        """First retained output of an inverse size decrease (default 0, the reference's window)."""
+        self._check(self._lib.fastfft_set_inverse_output_origin(self._h, ox, oy, oz))
+
     def SetOutputDtype(self, dtype):
         self._check(self._lib.fastfft_set_output_dtype(self._h, _dtype_code(dtype, _REAL_DTYPES)))
 

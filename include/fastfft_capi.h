@@ -88,6 +88,11 @@ FASTFFT_API fastfft_status fastfft_set_inverse_plan(fastfft_handle h, size_t ix,
 
 /* Work stream; NULL selects cudaStreamPerThread (the reference's only stream, usage.md:13). */
 FASTFFT_API fastfft_status fastfft_set_stream(fastfft_handle h, void* cuda_stream);
+/* First retained output (x, y, z) of an inverse size decrease; default (0, 0, 0), the
+ * reference's origin-anchored window.  (N - W) / 2 per axis keeps the central W.  The
+ * batched correlation's reduced-size path needs the origin at 0 and falls back to the
+ * size-N kernels otherwise.  No reference counterpart. */
+FASTFFT_API fastfft_status fastfft_set_inverse_output_origin(fastfft_handle h, size_t ox, size_t oy, size_t oz);
 /* Real output dtype of InvFFT / FwdImageInvFFT (default: input_dtype, as in the reference). */
 FASTFFT_API fastfft_status fastfft_set_output_dtype(fastfft_handle h, int dtype);
 
