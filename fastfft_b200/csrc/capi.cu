@@ -109,7 +109,8 @@ fastfft_status validate(fastfft_plan_s* h) {
     if (!in_range(nx) || !in_range(ny) || (dim == 3 && !in_range(nz)))
         return fail(h, FASTFFT_ERR_UNSUPPORTED, "transform sizes must be in [16, 8192]");
     if (!in_range(ii.x) || !in_range(ii.y)) return fail(h, FASTFFT_ERR_UNSUPPORTED, "transform sizes must be in [16, 8192]");
-    if (h->org_x + io.x > ii.x || h->org_y + io.y > ii.y || h->org_z + io.z > ii.z)
+    if (h->inv_change != SizeChange::Increase &&
+        (h->org_x + io.x > ii.x || h->org_y + io.y > ii.y || h->org_z + io.z > ii.z))
         return fail(h, FASTFFT_ERR_INVALID_DIMS, "inverse output window exceeds the transform (origin + size > N)");
     h->validated = true;
     return FASTFFT_OK;
