@@ -63,6 +63,8 @@ SIGNATURES = {
     "fastfft_fwd_image_inv_many": (_st, [Handle, ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                                          ctypes.POINTER(_vp), _op, _op, _op]),
     "fastfft_launch_count": (_st, [Handle, _ll]),
+    "fastfft_fwd_image_inv_2d_noalloc": (_st, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, _vp,
+                                               ctypes.c_int, ctypes.c_int, _op, _op, _op, _vp]),
     "fastfft_set_full_size_correlation": (_st, [Handle, ctypes.c_int]),
     "fastfft_correlation_size": (_st, [Handle, _dims]),
     "fastfft_profile_start": (_st, [Handle, ctypes.c_int]),

@@ -462,6 +462,11 @@ fastfft_status seq_xcorr(fastfft_plan_s* h, const void* in, const void* img, voi
 
 }  // namespace
 
+namespace ffb {
+// Message for fastfft_last_error(NULL) from entry points that take no handle.
+void set_unbound_error(const char* msg) { g_null_handle_error = msg; }
+}  // namespace ffb
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------

@@ -27,6 +27,9 @@ size_t xcorr_cols_smem(int n, int img_dtype, int L, int n_batch);
 // Device-wide FP64-generated twiddle table (generated once per device).
 cudaError_t twiddles_for(int n, const float2** out);
 
+// Message returned by fastfft_last_error(NULL), for entry points without a handle.
+void set_unbound_error(const char* msg);
+
 // Sets cudaFuncAttributeMaxDynamicSharedMemorySize once per (kernel, device).
 cudaError_t ensure_smem_attr(const void* func, size_t bytes, std::atomic<unsigned long long>* done_mask);
 

@@ -131,6 +131,29 @@ FASTFFT_API fastfft_status fastfft_set_full_size_correlation(fastfft_handle h, i
 /* Transform size {x, y} that fastfft_fwd_image_inv_many uses for this plan. */
 FASTFFT_API fastfft_status fastfft_correlation_size(fastfft_handle h, int dims[2]);
 
+/* 2D padded cross-correlation that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot allocate where they correlate: code inside a host
+ * application whose memory pool owns the GPU's free memory, and steady-state loops that
+ * must not stall on cudaMalloc/cudaFree (both synchronise the device).  The result is
+ * the one FwdImageInvFFT gives for a plan (in_x, in_y, 1) -> (n_x, n_y, 1) ->
+ * (out_x, out_y, 1) with a forward pad (or no change) and an inverse crop at the origin
+ * (or no change): FP32 template rows of pitch 2*(in_x/2+1), a complex64 (float2) image
+ * spectrum [kx][ky], an FP32 window of pitch 2*(out_x/2+1).
+ * Limit: its two intermediate arrays live in one fixed device array of 24 MiB that
+ * every GPU loading the library holds until exit; sizes with
+ * (n_x/2+1) * (round_up(in_y,4) + round_up(out_y,4)) * 8 bytes above it are rejected
+ * with FASTFFT_ERR_UNSUPPORTED (4096^2 with a 384-row template and a 1024-row window
+ * fits).  The first call on a device looks up that array's address and builds the
+ * twiddle table (it synchronises), so make it before any stream capture.  All calls share
+ * the array and it keeps the last call's contents (every value a call reads is written
+ * by that call first): calls that overlap on the GPU race.  cuda_stream NULL selects
+ * cudaStreamPerThread.  Errors: fastfft_last_error(NULL). */
+FASTFFT_API fastfft_status fastfft_fwd_image_inv_2d_noalloc(const float* input, int in_x, int in_y,
+                                                            const void* image_spectrum, int n_x, int n_y,
+                                                            float* output, int out_x, int out_y,
+                                                            const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                                            const fastfft_op* post_op, void* cuda_stream);
+
 /* ReturnInputMemorySize / ReturnFwdOutputMemorySize / ReturnInvOutputMemorySize
  * (FastFFT.h:194-204): element counts of InputType, FFTW-padded. */
 FASTFFT_API fastfft_status fastfft_input_memory_size(fastfft_handle h, long long* n);
