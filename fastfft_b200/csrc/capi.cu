@@ -165,7 +165,7 @@ void size_buffers(fastfft_plan_s* h) {
             h->off_c_real = round_up(stage, 256);
             h->off_c_spec = h->off_c_real + round_up(real, 256);
             // templates per launch: bounded by the shared memory of the fused column kernel
-            h->red_batch = ffb::kMaxBatch < 8 ? ffb::kMaxBatch : 8;
+            h->red_batch = h->red_batch_request;
             while (h->red_batch > 1 &&
                    xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, h->red_batch) > 227 * 1024)
                 h->red_batch--;
@@ -406,6 +406,25 @@ fastfft_status seq_inv(fastfft_plan_s* h, const void* in, int in_dtype, void* ou
     FFB_TRY(stage_cols(h, nz, ST_INV, FASTFFT_DTYPE_C64, cz));
     // x: rows r = z' * Wy + y'
     return stage_c2r(h, nx, region_b(h), h->pitch_b, (int)(wz * wy), out, 2LL * io.w, (int)io.x, (int)h->org_x,
+                     post_scale);
+}
+
+// 2D size-N fused correlation of one template of size (lx, ly) <= the plan's input size.
+fastfft_status seq_xcorr_sized(fastfft_plan_s* h, const void* in, int lx, int ly, const void* img, void* out,
+                               float pre_scale, const fastfft_op* intra_op, float post_scale) {
+    const Dims &fo = h->fwd_out, &io = h->inv_out;
+    const int nx = (int)fo.x, ny = (int)fo.y;
+    const int kw = nx / 2 + 1;
+    const long long pitch = 2LL * ((lx + (lx % 2 == 0 ? 2 : 1)) / 2);
+    FFB_TRY(stage_r2c(h, nx, h->input_dtype, in, pitch, ly, ly, 1, lx, region_a(h), h->pitch_a, kw, pre_scale));
+    ColArgs c = col_args(region_a(h), h->pitch_a, ly, region_b(h), h->pitch_b, (int)io.y, kw);
+    c.img = img;
+    c.img_stride = ny;
+    c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
+    c.intra_scale = intra_op ? intra_op->scale : 1.f;
+    c.W0 = (int)h->org_y;
+    FFB_TRY(stage_cols(h, ny, ST_XCORR, h->image_dtype, c));
+    return stage_c2r(h, nx, region_b(h), h->pitch_b, (int)io.y, out, 2LL * io.w, (int)io.x, (int)h->org_x,
                      post_scale);
 }
 
@@ -679,8 +698,8 @@ static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spec
 
 // Up to kMaxBatch templates through the reduced-size correlation against the prepared
 // spectrum: three launches whose grid.y runs over the templates.
-static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const* inputs, void* const* outs,
-                                      const fastfft_op* pre_op, const fastfft_op* intra_op,
+static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const* inputs, const int* dims,
+                                      void* const* outs, const fastfft_op* pre_op, const fastfft_op* intra_op,
                                       const fastfft_op* post_op) {
     const int mx = (int)h->red_mx, my = (int)h->red_my;
     char* c0 = region_c(h);
@@ -698,6 +717,13 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const
     a.in_pitch = 2LL * h->fwd_in.w; a.n_rows = (int)h->fwd_in.y; a.L = (int)h->fwd_in.x;
     a.out = t1; a.out_pitch = h->pitch_a; a.out_batch_stride = h->red_t1_stride;
     a.kmax = mx / 2 + 1; a.scale = scale_of(pre_op); a.tw = tw;
+    if (dims) {
+        for (int g = 0; g < n; g++) {
+            a.L_g[g] = dims[2 * g];
+            a.rows_g[g] = dims[2 * g + 1];
+            a.pitch_g[g] = 2LL * ((dims[2 * g] + (dims[2 * g] % 2 == 0 ? 2 : 1)) / 2);
+        }
+    }
     if ((e = launch_r2c_rows(mx, h->input_dtype, a, h->stream)) != cudaSuccess) return cuda_fail(h, e, "r2c row pass");
     h->launches++;
     prof_mark(h);
@@ -708,6 +734,8 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const
     c.img = spec; c.img_stride = my;
     c.out = t2; c.out_pitch = h->pitch_b; c.out_batch = h->red_t2_stride; c.W = (int)h->inv_out.y;
     c.n_cols = mx / 2 + 1; c.n_batch = n;
+    if (dims)
+        for (int g = 0; g < n; g++) c.L_g[g] = dims[2 * g + 1];
     c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
     c.intra_scale = intra_op ? intra_op->scale : 1.f;
     c.tw = tw; c.err = h->dev_err;
@@ -739,11 +767,10 @@ fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const 
     return xcorr_one(h, input, image_spectrum, output ? output : const_cast<void*>(input), pre_op, intra_op, post_op);
 }
 
-fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, const void* const* inputs,
-                                          const void* const* image_spectra, void* const* outputs,
-                                          const fastfft_op* pre_op, const fastfft_op* intra_op,
-                                          const fastfft_op* post_op) {
-    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+// Shared body of the batched calls; dims (x, y per template) may be NULL (plan size).
+static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inputs, const int* dims,
+                                 const void* const* image_spectra, void* const* outputs, const fastfft_op* pre_op,
+                                 const fastfft_op* intra_op, const fastfft_op* post_op) {
     if (n < 0 || (n > 0 && (!inputs || !image_spectra)))
         return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image array");
     for (int i = 0; i < n; i++)
@@ -751,19 +778,34 @@ fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, const void* c
             return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image pointer in the batch");
     fastfft_status st = xcorr_checks(h, pre_op, intra_op, post_op);
     if (st != FASTFFT_OK) return st;
+    if (dims) {
+        if (h->rank != 2) return fail(h, FASTFFT_ERR_UNSUPPORTED, "per-template sizes are 2D only");
+        for (int i = 0; i < n; i++)
+            if (dims[2 * i] < 1 || dims[2 * i + 1] < 1 || dims[2 * i] > h->fwd_in.x || dims[2 * i + 1] > h->fwd_in.y)
+                return fail(h, FASTFFT_ERR_INVALID_DIMS,
+                            "template " + std::to_string(i) + " is larger than the plan's forward input size");
+    }
     if (!h->red_ok || h->force_full_size) {
         for (int i = 0; i < n; i++) {
             void* out = (outputs && outputs[i]) ? outputs[i] : const_cast<void*>(inputs[i]);
-            st = xcorr_one(h, inputs[i], image_spectra[i], out, pre_op, intra_op, post_op);
+            if (dims) {
+                prof_begin_call(h);
+                st = seq_xcorr_sized(h, inputs[i], dims[2 * i], dims[2 * i + 1], image_spectra[i], out,
+                                     scale_of(pre_op), intra_op, scale_of(post_op));
+                prof_end_call(h);
+            } else {
+                st = xcorr_one(h, inputs[i], image_spectra[i], out, pre_op, intra_op, post_op);
+            }
             if (st != FASTFFT_OK) return st;
         }
         return FASTFFT_OK;
     }
     // Reduced-size path: templates are grouped by image (in order of first use); each
-    // distinct image is prepared once for the whole call.
+    // distinct image is prepared once for the whole call; up to red_batch templates per launch.
     std::vector<char> done(n, 0);
     const void* grp_in[kMaxBatch];
     void* grp_out[kMaxBatch];
+    int grp_dims[2 * kMaxBatch];
     for (int i = 0; i < n; i++) {
         if (done[i]) continue;
         const void* img = image_spectra[i];
@@ -774,18 +816,64 @@ fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, const void* c
             if (done[k] || image_spectra[k] != img) continue;
             grp_in[m] = inputs[k];
             grp_out[m] = (outputs && outputs[k]) ? outputs[k] : const_cast<void*>(inputs[k]);
+            if (dims) {
+                grp_dims[2 * m] = dims[2 * k];
+                grp_dims[2 * m + 1] = dims[2 * k + 1];
+            }
             done[k] = 1;
             if (++m == h->red_batch) {
-                st = red_xcorr_batch(h, m, grp_in, grp_out, pre_op, intra_op, post_op);
+                st = red_xcorr_batch(h, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op, post_op);
                 if (st != FASTFFT_OK) return st;
                 m = 0;
             }
         }
         if (m > 0) {
-            st = red_xcorr_batch(h, m, grp_in, grp_out, pre_op, intra_op, post_op);
+            st = red_xcorr_batch(h, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op, post_op);
             if (st != FASTFFT_OK) return st;
         }
     }
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, const void* const* inputs,
+                                          const void* const* image_spectra, void* const* outputs,
+                                          const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                          const fastfft_op* post_op) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    return xcorr_many(h, n, inputs, nullptr, image_spectra, outputs, pre_op, intra_op, post_op);
+}
+
+fastfft_status fastfft_fwd_image_inv_many_sized(fastfft_handle h, int n, const void* const* inputs,
+                                                const int* template_dims, const void* const* image_spectra,
+                                                void* const* outputs, const fastfft_op* pre_op,
+                                                const fastfft_op* intra_op, const fastfft_op* post_op) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (n > 0 && !template_dims) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null template size array");
+    return xcorr_many(h, n, inputs, template_dims, image_spectra, outputs, pre_op, intra_op, post_op);
+}
+
+fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (n < 1 || n > kMaxBatch) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "templates per launch must be in [1, 16]");
+    h->red_batch_request = n;
+    h->validated = false;
+    if (h->fwd_set && h->inv_set) {
+        fastfft_status st = validate(h);
+        if (st != FASTFFT_OK) return st;
+        const size_t before = h->buffer_bytes;
+        size_buffers(h);
+        if (h->buffer && (size_t)(h->bytes_a + h->bytes_b + h->bytes_c) + 256 > before) {
+            cudaFree(h->buffer);
+            h->buffer = nullptr;
+            h->buffer_bytes = 0;
+        }
+    }
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_templates_per_launch(fastfft_handle h, int* n) {
+    if (!h || !n) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null argument");
+    *n = h->red_ok && !h->force_full_size ? h->red_batch : 1;
     return FASTFFT_OK;
 }
 

@@ -91,6 +91,10 @@ struct RowFwdArgs {
     // [kx][y][z] has z contiguous.  rows_z <= 1: row r reads input row r.
     int rows_y;
     int rows_z;
+    // Per-template sizes of a batch of uneven templates (0: use n_rows / L / in_pitch).
+    int rows_g[kMaxBatch];
+    int L_g[kMaxBatch];
+    long long pitch_g[kMaxBatch];
 };
 
 __device__ __forceinline__ long long input_row(int r, int rows_y, int rows_z) {
@@ -109,24 +113,28 @@ r2c_rows_kernel(RowFwdArgs a) {
     const int j = threadIdx.x - f * T;
     G g(smem, f);
     float2* s = g.base;
+    const int gb = blockIdx.y;
+    const int n_rows = a.rows_g[gb] > 0 ? a.rows_g[gb] : a.n_rows;
+    const int L = a.L_g[gb] > 0 ? a.L_g[gb] : a.L;
+    const long long in_pitch = a.pitch_g[gb] > 0 ? a.pitch_g[gb] : a.in_pitch;
     const int ra = 2 * (blockIdx.x * FPB + f);
-    const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
-    const InT* in_g = static_cast<const InT*>(a.in[blockIdx.y]);
-    const InT* pa = in_g + input_row(ra, a.rows_y, a.rows_z) * a.in_pitch;
-    const InT* pb = in_g + input_row(ra + 1, a.rows_y, a.rows_z) * a.in_pitch;
+    const bool has_a = ra < n_rows, has_b = ra + 1 < n_rows;
+    const InT* in_g = static_cast<const InT*>(a.in[gb]);
+    const InT* pa = in_g + input_row(ra, a.rows_y, a.rows_z) * in_pitch;
+    const InT* pb = in_g + input_row(ra + 1, a.rows_y, a.rows_z) * in_pitch;
     float2* const out_g = a.out + (long long)blockIdx.y * a.out_batch_stride;
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
         const int n = j + T * q;
         float xa = 0.f, xb = 0.f;
-        if (n < a.L) {
+        if (n < L) {
             if (has_a) xa = ld_real<InT>(pa + n);
             if (has_b) xb = ld_real<InT>(pb + n);
         }
         v[q] = make_float2(xa * a.scale, xb * a.scale);
     }
-    BlockFft<N, false>::run(v, g, j, a.tw, leading_slots<T>(a.L, j));
+    BlockFft<N, false>::run(v, g, j, a.tw, leading_slots<T>(L, j));
 
     // Split Z = A + iB into the two real-row spectra: A[k] = (Z[k] + conj Z[N-k]) / 2,
     // B[k] = -i (Z[k] - conj Z[N-k]) / 2.
@@ -135,7 +143,11 @@ r2c_rows_kernel(RowFwdArgs a) {
     for (int q = 0; q < 16; q++) s[phys(j + T * q)] = v[q];
     __syncthreads();
     const int items = FPB * a.kmax;
-    for (int i = threadIdx.x; i < items; i += blockDim.x) {
+    constexpr int kItemsPerThread = (FPB * (N / 2 + 1) + T * FPB - 1) / (T * FPB);
+#pragma unroll
+    for (int it = 0; it < kItemsPerThread; it++) {
+        const int i = threadIdx.x + it * (T * FPB);
+        if (i >= items) continue;
         const int ff = i % FPB;
         const int k = i / FPB;
         const float2* sf = smem + ff * G::STRIDE;
@@ -145,9 +157,9 @@ r2c_rows_kernel(RowFwdArgs a) {
         const float2 B = make_float2(0.5f * (z1.y + z2.y), 0.5f * (z2.x - z1.x));
         const int rr = 2 * (blockIdx.x * FPB + ff);
         float2* o = out_g + (long long)k * a.out_pitch + rr;
-        if (rr + 1 < a.n_rows) {
+        if (rr + 1 < n_rows) {
             *reinterpret_cast<float4*>(o) = make_float4(A.x, A.y, B.x, B.y);
-        } else if (rr < a.n_rows) {
+        } else if (rr < n_rows) {
             *o = A;
         }
     }
@@ -281,26 +293,42 @@ c2r_rows_kernel(RowInvArgs a) {
     // Gather rows (2 per FFT) and build Z[k] = A[k] + i B[k] over the full circle
     // from the half spectrum (A, B Hermitian).  The imaginary parts of the k = 0
     // and k = N/2 bins are dropped, as a C2R of a Hermitian spectrum does.
+    // (H + 1) / T <= 9 items per thread: all of a thread's loads are issued before any of
+    // them is used, so they are in flight together.
     const int items = FPB * (H + 1);
-    for (int i = threadIdx.x; i < items; i += blockDim.x) {
+    constexpr int kItemsPerThread = (FPB * (H + 1) + T * FPB - 1) / (T * FPB);
+    float4 ld[kItemsPerThread];
+#pragma unroll
+    for (int it = 0; it < kItemsPerThread; it++) {
+        const int i = threadIdx.x + it * (T * FPB);
         const int ff = i % FPB;
         const int k = i / FPB;
         const int rr = 2 * (blockIdx.x * FPB + ff);
-        float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
         const float2* p = a.in + (long long)blockIdx.y * a.in_batch_stride + (long long)k * a.in_pitch + rr;
-        if (rr + 1 < a.n_rows) {
-            const float4 t = *reinterpret_cast<const float4*>(p);
-            A = make_float2(t.x, t.y);
-            B = make_float2(t.z, t.w);
-        } else if (rr < a.n_rows) {
-            A = *p;
+        ld[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (i < items) {
+            if (rr + 1 < a.n_rows) {
+                ld[it] = *reinterpret_cast<const float4*>(p);
+            } else if (rr < a.n_rows) {
+                const float2 t = *p;
+                ld[it] = make_float4(t.x, t.y, 0.f, 0.f);
+            }
         }
-        float2* sf = smem + ff * G::STRIDE;
-        if (k == 0 || k == H) {
-            sf[phys(k)] = make_float2(A.x, B.x);
-        } else {
-            sf[phys(k)] = make_float2(A.x - B.y, A.y + B.x);
-            sf[phys(N - k)] = make_float2(A.x + B.y, B.x - A.y);
+    }
+#pragma unroll
+    for (int it = 0; it < kItemsPerThread; it++) {
+        const int i = threadIdx.x + it * (T * FPB);
+        if (i < items) {
+            const int ff = i % FPB;
+            const int k = i / FPB;
+            const float2 A = make_float2(ld[it].x, ld[it].y), B = make_float2(ld[it].z, ld[it].w);
+            float2* sf = smem + ff * G::STRIDE;
+            if (k == 0 || k == H) {
+                sf[phys(k)] = make_float2(A.x, B.x);
+            } else {
+                sf[phys(k)] = make_float2(A.x - B.y, A.y + B.x);
+                sf[phys(N - k)] = make_float2(A.x + B.y, B.x - A.y);
+            }
         }
     }
     __syncthreads();

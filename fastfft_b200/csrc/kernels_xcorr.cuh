@@ -104,6 +104,7 @@ struct XcorrColArgs {
     float intra_scale;
     const float2* tw;
     int* err;
+    int L_g[kMaxBatch];        // per-template valid rows of uneven batches (0: use L)
 };
 
 // Shared-memory plan of the kernel (bytes), shared by the host launcher.
@@ -149,12 +150,14 @@ xcorr_cols_kernel(XcorrColArgs a) {
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         fence_barrier_init();
-        const uint32_t bytes = (uint32_t)(SM::kImgBytes + a.n_batch * lcol * 8);
+        uint32_t bytes = (uint32_t)SM::kImgBytes;
+        for (int g = 0; g < a.n_batch; g++) bytes += (uint32_t)SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8;
         mbar_arrive_expect_tx(bar, bytes);
         bulk_g2s(sm_raw + SM::img_off(), static_cast<const ImgC*>(a.img) + (long long)col * a.img_stride,
                  SM::kImgBytes, bar);
         for (int g = 0; g < a.n_batch; g++)
-            bulk_g2s(t1_s + g * lcol, a.t1 + g * a.t1_batch + (long long)col * a.t1_pitch, lcol * 8, bar);
+            bulk_g2s(t1_s + g * lcol, a.t1 + g * a.t1_batch + (long long)col * a.t1_pitch,
+                     SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8, bar);
     }
     __syncthreads();  // barrier initialised before anyone polls it
     if (!mbar_wait(bar, 0)) {
@@ -171,6 +174,7 @@ xcorr_cols_kernel(XcorrColArgs a) {
     for (int it = 0; it < rounds; it++) {
         const int g = it * FPB + f;
         const bool live = g < a.n_batch;
+        const int Lg = (live && a.L_g[g] > 0) ? a.L_g[g] : a.L;
         // keep the next template's loads from being scheduled into this template's
         // transforms (that would hold twice the values live and spill)
         asm volatile("" ::: "memory");
@@ -179,9 +183,9 @@ xcorr_cols_kernel(XcorrColArgs a) {
 #pragma unroll
         for (int q = 0; q < 16; q++) {
             const int n = j + T * q;
-            v[q] = (live && n < a.L) ? src[n] : make_float2(0.f, 0.f);
+            v[q] = (live && n < Lg) ? src[n] : make_float2(0.f, 0.f);
         }
-        BlockFft<N, false>::run(v, grp, j, a.tw, live ? leading_slots<T>(a.L, j) : 0);
+        BlockFft<N, false>::run(v, grp, j, a.tw, live ? leading_slots<T>(Lg, j) : 0);
         if constexpr (MUL) {
 #pragma unroll
             for (int q = 0; q < 16; q++) {

@@ -55,6 +55,7 @@ struct fastfft_plan_s {
     long long off_c_real = 0, off_c_spec = 0;
     bool force_full_size = false;  // fastfft_set_full_size_correlation
     int red_batch = 8;              // templates per launch in the reduced-size path
+    int red_batch_request = 8;      // fastfft_set_templates_per_launch (bounded by shared memory)
     long long red_t1_stride = 0, red_t2_stride = 0;  // complex elements per template slice
     long long off_c_t1 = 0, off_c_t2 = 0;
     int* dev_err = nullptr;  // device status word of bounded waits (inside the work buffer)

@@ -158,6 +158,33 @@ class FourierTransformer:
         self._check(self._lib.fastfft_fwd_image_inv_many(self._h, n, ins, ims, outs, _opref(pre_op), _opref(intra_op),
                                                          _opref(post_op)))
 
+    def FwdImageInvFFTManySized(self, inputs, sizes, images, outputs=None, pre_op=None, intra_op=None,
+                                post_op=None):
+        """FwdImageInvFFTMany for templates of uneven sizes: sizes[i] = (x, y) of template i."""
+        n = len(inputs)
+        if not isinstance(images, (list, tuple)):
+            images = [images] * n
+        if len(sizes) != n or len(images) != n or (outputs is not None and len(outputs) != n):
+            raise ValueError("inputs, sizes, images and outputs must have the same length")
+        if intra_op is None:
+            intra_op = KernelFunction.conj_mul()
+        arr = ctypes.c_void_p * n
+        dims = (ctypes.c_int * (2 * n))(*[int(v) for xy in sizes for v in xy])
+        ins = arr(*[_ptr(x) for x in inputs])
+        ims = arr(*[_ptr(x) for x in images])
+        outs = arr(*[_ptr(x) for x in outputs]) if outputs is not None else None
+        self._bind_stream()
+        self._check(self._lib.fastfft_fwd_image_inv_many_sized(self._h, n, ins, dims, ims, outs, _opref(pre_op),
+                                                               _opref(intra_op), _opref(post_op)))
+
+    def SetTemplatesPerLaunch(self, n):
+        self._check(self._lib.fastfft_set_templates_per_launch(self._h, int(n)))
+
+    def TemplatesPerLaunch(self):
+        v = ctypes.c_int()
+        self._check(self._lib.fastfft_templates_per_launch(self._h, ctypes.byref(v)))
+        return v.value
+
     def SetFullSizeCorrelation(self, force=True):
         """Make FwdImageInvFFTMany use the size-N kernels even when a smaller size is exact."""
         self._check(self._lib.fastfft_set_full_size_correlation(self._h, int(bool(force))))

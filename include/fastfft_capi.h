@@ -120,6 +120,20 @@ FASTFFT_API fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, c
                                                       const fastfft_op* pre_op, const fastfft_op* intra_op,
                                                       const fastfft_op* post_op);
 
+/* fastfft_fwd_image_inv_many for templates of uneven sizes: template i is
+ * template_dims[2i] x template_dims[2i+1] (x, y), no larger than the plan's forward input
+ * size, with rows of pitch 2*(x/2+1); all share the plan's transform and window.  The
+ * reference plans one size per FourierTransformer; no counterpart. */
+FASTFFT_API fastfft_status fastfft_fwd_image_inv_many_sized(fastfft_handle h, int n, const void* const* inputs,
+                                                            const int* template_dims,
+                                                            const void* const* image_spectra, void* const* outputs,
+                                                            const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                                            const fastfft_op* post_op);
+/* Templates per launch of the batched reduced-size path (1..16, default 8; lowered if the
+ * fused column kernel's shared memory would not fit), and the value in effect. */
+FASTFFT_API fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n);
+FASTFFT_API fastfft_status fastfft_templates_per_launch(fastfft_handle h, int* n);
+
 /* The batched call correlates at the smallest power-of-two size M >= L + W - 1 per axis
  * when that is below the plan's N (template in [0, L), window in [0, W)): every
  * retained lag then reads image pixels in [0, L + W - 1) only, so the size-M

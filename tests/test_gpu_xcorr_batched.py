@@ -109,3 +109,55 @@ def test_many_low_precision_image(torch_cuda, img_dt):
     p = O.Plan(fin, fout, fout, iout)
     ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), spec_deq, p, out_dtype=np.float64), iout)
     assert O.rel_l2(O.real_from_padded(host(out), iout), ref) <= RTOL_L2_FP32
+
+
+@pytest.mark.parametrize("force_full", [False, True])
+def test_many_sized_uneven_templates(torch_cuda, force_full):
+    """Uneven template sizes in one call (one plan for the largest), against the oracle."""
+    torch = torch_cuda
+    fmax, fout, iout = (96, 96, 1), (1024, 1024, 1), (128, 128, 1)
+    ft = plan(fmax, fout, iout)
+    ft.SetFullSizeCorrelation(force_full)
+    assert ft.CorrelationSize() == ((1024, 1024) if force_full else (256, 256))
+    spec = image_spectrum(fout, 12)
+    d_spec = dev(torch, spec.view(np.float32))
+    rng = np.random.default_rng(13)
+    sizes = [(32, 32), (96, 96), (48, 64), (96, 40), (64, 64), (17, 95), (96, 96), (33, 33), (80, 20), (64, 96)]
+    ts = [rng.standard_normal((y, x)).astype(np.float32) for x, y in sizes]
+    ins = [dev(torch, O.real_to_padded(t, (x, y, 1))) for t, (x, y) in zip(ts, sizes)]
+    outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    ft.FwdImageInvFFTManySized(ins, sizes, d_spec, outs)
+    for t, (x, y), o in zip(ts, sizes, outs):
+        p = O.Plan((x, y, 1), fout, fout, iout)
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, (x, y, 1)), spec, p, out_dtype=np.float64), iout)
+        got = O.real_from_padded(host(o), iout)
+        assert O.rel_l2(got, ref) <= RTOL_L2_FP32, (x, y)
+
+
+def test_many_sized_rejects_oversized_template(torch_cuda):
+    ft = plan((64, 64, 1), (512, 512, 1), (64, 64, 1))
+    t = torch_cuda.zeros(8192, device="cuda")
+    spec = torch_cuda.zeros(2 * 257 * 512, device="cuda")
+    out = torch_cuda.zeros(66 * 64, device="cuda")
+    with pytest.raises(F.FastFFTError) as e:
+        ft.FwdImageInvFFTManySized([t], [(65, 64)], spec, [out])
+    assert "larger than the plan" in str(e.value)
+
+
+@pytest.mark.parametrize("per_launch", [1, 3, 16])
+def test_templates_per_launch_setting(torch_cuda, per_launch):
+    torch = torch_cuda
+    fin, fout, iout = (40, 40, 1), (512, 512, 1), (64, 64, 1)
+    ft = plan(fin, fout, iout)
+    ft.SetTemplatesPerLaunch(per_launch)
+    assert ft.TemplatesPerLaunch() == per_launch
+    spec = image_spectrum(fout, 21)
+    d_spec = dev(torch, spec.view(np.float32))
+    rng = np.random.default_rng(2)
+    ts = [rng.standard_normal((40, 40)).astype(np.float32) for _ in range(7)]
+    outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    ft.FwdImageInvFFTMany([dev(torch, O.real_to_padded(t, fin)) for t in ts], d_spec, outs)
+    p = O.Plan(fin, fout, fout, iout)
+    for t, o in zip(ts, outs):
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), spec, p, out_dtype=np.float64), iout)
+        assert O.rel_l2(O.real_from_padded(host(o), iout), ref) <= RTOL_L2_FP32
