@@ -6,6 +6,6 @@ computed by hand-written CUDA kernels in libfastfft_b200.so (C ABI:
 include/fastfft_capi.h).
 """
 from ._capi import FastFFTError, LIB_PATH
-from .transformer import FourierTransformer, KernelFunction
+from .transformer import FourierTransformer, KernelFunction, decode_peaks
 
-__all__ = ["FourierTransformer", "KernelFunction", "FastFFTError", "LIB_PATH"]
+__all__ = ["FourierTransformer", "KernelFunction", "FastFFTError", "LIB_PATH", "decode_peaks"]

@@ -276,7 +276,21 @@ struct RowInvArgs {
     const float2* tw;
     int n_batch;           // batch entries in this launch (grid.y)
     int X0;
+    // Fused peak search: if peaks is set, batch entry g's maximum over the retained
+    // window and its first flat index (row * W + x) are folded into peaks[g] as a
+    // peak_key(); with peaks_only the window itself is not written.
+    unsigned long long* peaks;
+    int peaks_only;
+    int peak_slot[kMaxBatch];  // batch entry g folds into peaks[peak_slot[g]]
 };
+
+// Total order on (value, index) for a 64-bit atomicMax: larger value wins, and among
+// equal values the smaller index (the first occurrence, as argmax returns it).
+__device__ __forceinline__ unsigned long long peak_key(float v, unsigned int index) {
+    const unsigned int b = __float_as_uint(v);
+    const unsigned int ordered = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    return ((unsigned long long)ordered << 32) | (0xFFFFFFFFu - index);
+}
 
 template <int N, class OutT, int FPB>
 __global__ void __launch_bounds__(FftShape<N>::T * FPB)
@@ -340,13 +354,38 @@ c2r_rows_kernel(RowInvArgs a) {
     OutT* oa = static_cast<OutT*>(a.out[blockIdx.y]) + (long long)ra * a.out_pitch;
     OutT* ob = oa + a.out_pitch;
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
+    if (!a.peaks_only) {
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-        const int n = j + T * q - a.X0;
-        if (n >= 0 && n < a.W) {
-            if (has_a) st_real<OutT>(oa + n, v[q].x * a.scale);
-            if (has_b) st_real<OutT>(ob + n, v[q].y * a.scale);
+        for (int q = 0; q < 16; q++) {
+            const int n = j + T * q - a.X0;
+            if (n >= 0 && n < a.W) {
+                if (has_a) st_real<OutT>(oa + n, v[q].x * a.scale);
+                if (has_b) st_real<OutT>(ob + n, v[q].y * a.scale);
+            }
         }
+    }
+    if (a.peaks) {
+        unsigned long long best = 0;
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int n = j + T * q - a.X0;
+            if (n >= 0 && n < a.W) {
+                if (has_a) {
+                    const unsigned long long k = peak_key(v[q].x * a.scale, (unsigned)(ra * a.W + n));
+                    best = k > best ? k : best;
+                }
+                if (has_b) {
+                    const unsigned long long k = peak_key(v[q].y * a.scale, (unsigned)((ra + 1) * a.W + n));
+                    best = k > best ? k : best;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+            best = other > best ? other : best;
+        }
+        if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(a.peaks + a.peak_slot[blockIdx.y], best);
     }
 }
 

@@ -64,6 +64,17 @@ def _opref(op):
     return ctypes.byref(op) if op is not None else None
 
 
+def decode_peaks(peaks):
+    """(values float32, flat indices int64) of keys written by FwdImageInvFFTManyPeaks (host numpy)."""
+    import numpy as np
+
+    k = np.asarray(peaks.cpu() if hasattr(peaks, "cpu") else peaks).astype(np.int64).view(np.uint64)
+    ordered = (k >> np.uint64(32)).astype(np.uint32)
+    bits = np.where(ordered & np.uint32(0x80000000), ordered & np.uint32(0x7FFFFFFF), ~ordered).astype(np.uint32)
+    index = (np.uint64(0xFFFFFFFF) - (k & np.uint64(0xFFFFFFFF))).astype(np.int64)
+    return bits.view(np.float32), index
+
+
 class FourierTransformer:
     def __init__(self, compute_dtype="float32", input_dtype="float32", image_dtype="complex64", rank=2):
         self._lib = C.lib()
@@ -176,6 +187,28 @@ class FourierTransformer:
         self._bind_stream()
         self._check(self._lib.fastfft_fwd_image_inv_many_sized(self._h, n, ins, dims, ims, outs, _opref(pre_op),
                                                                _opref(intra_op), _opref(post_op)))
+
+    def FwdImageInvFFTManyPeaks(self, inputs, images, peaks, sizes=None, outputs=None, pre_op=None, intra_op=None,
+                                post_op=None):
+        """Batched correlation with a fused peak search into `peaks` (int64 CUDA tensor, one per
+        template; decode with decode_peaks).  outputs None: the windows are not written."""
+        n = len(inputs)
+        if not isinstance(images, (list, tuple)):
+            images = [images] * n
+        if len(images) != n or (outputs is not None and len(outputs) != n) or (sizes is not None and len(sizes) != n):
+            raise ValueError("inputs, images, sizes and outputs must have the same length")
+        if peaks.numel() < n or peaks.element_size() != 8:
+            raise ValueError("peaks must hold one 64-bit value per template")
+        if intra_op is None:
+            intra_op = KernelFunction.conj_mul()
+        arr = ctypes.c_void_p * n
+        dims = (ctypes.c_int * (2 * n))(*[int(v) for xy in sizes for v in xy]) if sizes is not None else None
+        ins = arr(*[_ptr(x) for x in inputs])
+        ims = arr(*[_ptr(x) for x in images])
+        outs = arr(*[_ptr(x) for x in outputs]) if outputs is not None else None
+        self._bind_stream()
+        self._check(self._lib.fastfft_fwd_image_inv_many_peaks(self._h, n, ins, dims, ims, outs, _ptr(peaks),
+                                                               _opref(pre_op), _opref(intra_op), _opref(post_op)))
 
     def SetTemplatesPerLaunch(self, n):
         self._check(self._lib.fastfft_set_templates_per_launch(self._h, int(n)))

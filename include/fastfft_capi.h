@@ -129,6 +129,22 @@ FASTFFT_API fastfft_status fastfft_fwd_image_inv_many_sized(fastfft_handle h, in
                                                             const void* const* image_spectra, void* const* outputs,
                                                             const fastfft_op* pre_op, const fastfft_op* intra_op,
                                                             const fastfft_op* post_op);
+/* Batched correlation with a fused peak search: peaks[i] (device memory, n values)
+ * receives the maximum of template i's window and its first flat index
+ * y * out_x + x, packed as ((ordered float bits) << 32) | (0xFFFFFFFF - index), where
+ * ordered bits = bits | 0x80000000 for v >= 0 and ~bits for v < 0 (decode with
+ * fastfft_decode_peak).  outputs NULL: the windows are not written at all (the window
+ * write is the largest store of the correlation); otherwise they are written too.
+ * template_dims may be NULL (plan size).  No reference counterpart (the reference's
+ * callers search the returned window on their own). */
+FASTFFT_API fastfft_status fastfft_fwd_image_inv_many_peaks(fastfft_handle h, int n, const void* const* inputs,
+                                                            const int* template_dims,
+                                                            const void* const* image_spectra, void* const* outputs,
+                                                            unsigned long long* peaks, const fastfft_op* pre_op,
+                                                            const fastfft_op* intra_op, const fastfft_op* post_op);
+/* Host-side decode of one peaks[] entry. */
+FASTFFT_API void fastfft_decode_peak(unsigned long long key, float* value, unsigned int* index);
+
 /* Templates per launch of the batched reduced-size path (1..16, default 8; lowered if the
  * fused column kernel's shared memory would not fit), and the value in effect. */
 FASTFFT_API fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n);

@@ -161,3 +161,35 @@ def test_templates_per_launch_setting(torch_cuda, per_launch):
     for t, o in zip(ts, outs):
         ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), spec, p, out_dtype=np.float64), iout)
         assert O.rel_l2(O.real_from_padded(host(o), iout), ref) <= RTOL_L2_FP32
+
+
+@pytest.mark.parametrize("write_windows,force_full", [(False, False), (True, False), (False, True)])
+def test_many_peaks_match_oracle_argmax(torch_cuda, write_windows, force_full):
+    """Fused peak search: max and first-occurrence argmax of every window, bit-exact index."""
+    torch = torch_cuda
+    fin, fout, iout = (64, 64, 1), (1024, 1024, 1), (200, 150, 1)
+    ft = plan(fin, fout, iout)
+    ft.SetFullSizeCorrelation(force_full)
+    img = O.gaussian_blob_image(1024, n_blobs=6, seed=5)
+    spec = O.image_spectrum_fp32(img)
+    d_spec = dev(torch, spec.view(np.float32))
+    rng = np.random.default_rng(17)
+    sizes = [(64, 64), (40, 64), (64, 33), (20, 20), (64, 64), (50, 60)]
+    ts = [rng.standard_normal((y, x)).astype(np.float32) for x, y in sizes]
+    ins = [dev(torch, O.real_to_padded(t, (x, y, 1))) for t, (x, y) in zip(ts, sizes)]
+    outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts] if write_windows else None
+    peaks = torch.zeros(len(ts), dtype=torch.int64, device="cuda")
+    ft.FwdImageInvFFTManyPeaks(ins, d_spec, peaks, sizes=sizes, outputs=outs)
+    vals, idx = F.decode_peaks(peaks)
+    for i, (t, (x, y)) in enumerate(zip(ts, sizes)):
+        p = O.Plan((x, y, 1), fout, fout, iout)
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, (x, y, 1)), spec, p, out_dtype=np.float64),
+                                 iout)[0]
+        ri, rtop, margin = O.peak(ref)
+        if margin > 1e-4 * abs(rtop):
+            assert idx[i] == ri, i
+        assert abs(vals[i] - rtop) <= 1e-5 * abs(rtop)
+        if write_windows:
+            got = O.real_from_padded(host(outs[i]), iout)[0]
+            assert O.rel_l2(got, ref) <= RTOL_L2_FP32
+            assert O.peak(got)[0] == idx[i]
