@@ -204,6 +204,73 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------------------
+# Uneven batch: many template sizes against one resident image, one graph launch
+# ---------------------------------------------------------------------------
+UNEVEN_SIZES = (128, 192, 256, 384)
+UNEVEN_N_TEMPLATES = 1024
+UNEVEN_WINDOW = 512
+
+
+def run_uneven(dev, image_f32, storage="float32", reps=5):
+    """1024 templates with edges drawn uniformly from {128,192,256,384} (N(0,1), seeded),
+    zero-padded to 4096^2, correlated against one resident 4096^2 image spectrum, cropped
+    to 512^2 windows.  The whole batch is captured once in a CUDA graph and replayed.
+    storage "bfloat16": templates and image spectrum stored in BF16 (image scaled by 1/4096
+    before rounding), arithmetic in FP32."""
+    import torch
+
+    import fastfft_b200 as F
+    from fastfft_b200.autotune import tune
+
+    rng = np.random.default_rng(20261203 + 5)
+    edges = rng.choice(UNEVEN_SIZES, size=UNEVEN_N_TEMPLATES)
+    L, W = max(UNEVEN_SIZES), UNEVEN_WINDOW
+    tdt = torch.float32 if storage == "float32" else torch.bfloat16
+    ft = F.FourierTransformer(input_dtype=storage, image_dtype="complex64" if storage == "float32" else "complex_bf16")
+    ft.SetForwardFFTPlan(L, L, 1, N, N, 1)
+    ft.SetInverseFFTPlan(N, N, 1, W, W, 1)
+    ft.SetOutputDtype("float32")
+    if storage == "float32":
+        image = image_f32
+    else:
+        image = (image_f32 * (1.0 / N)).to(tdt)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(20261203 + 6)
+    ins, sizes = [], []
+    for e in edges:
+        e = int(e)
+        pitch = 2 * (e // 2 + 1)
+        t = torch.zeros(e, pitch, dtype=tdt, device=dev)
+        t[:, :e] = torch.randn(e, e, device=dev, generator=gen).to(tdt)
+        ins.append(t.view(-1))
+        sizes.append((e, e))
+    out = torch.empty(UNEVEN_N_TEMPLATES, ft.ReturnInvOutputMemorySize(), dtype=torch.float32, device=dev)
+    outs = [out[i] for i in range(UNEVEN_N_TEMPLATES)]
+    per_launch = tune(ft, ins, image, outs, sizes=sizes)
+    for _ in range(2):
+        ft.FwdImageInvFFTManySized(ins, sizes, image, outs)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        ft.FwdImageInvFFTManySized(ins, sizes, image, outs)
+    graph.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del graph
+    return {"workload": "1024 templates, edges uniform in {128,192,256,384}, zero-padded to 4096^2, one resident "
+                        "4096^2 image spectrum, 512^2 windows; the whole batch is one CUDA graph launch",
+            "storage": storage, "value": UNEVEN_N_TEMPLATES / (ms * 1e-3), "unit": UNIT, "ms_per_batch": ms,
+            "correlation_size": list(ft.CorrelationSize()), "templates_per_launch": per_launch,
+            "template_edge_counts": {str(k): int((edges == k).sum()) for k in UNEVEN_SIZES}}
+
+
+# ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
 def run_ours(args, world, rank, local):
@@ -323,25 +390,32 @@ def run_ours(args, world, rank, local):
     e2e_ms = max_over_ranks(world, f0.elapsed_time(f1), torch, dev)
     e2e_value = world * e2e_steps * B / (e2e_ms * 1e-3)
 
-    # the same through the fused peak search: 8 bytes per template come back
+    # the same through the fused peak search: 8 bytes per template come back; the next
+    # step's templates are uploaded on the copy stream while this step computes
     peaks = torch.zeros(B, dtype=torch.int64, device=dev)
     h_peaks = torch.empty(B, dtype=torch.int64, pin_memory=True)
+    d_tpl = [templates, torch.empty_like(templates)]
+    ins2 = [[d_tpl[k][i] for i in range(B)] for k in range(2)]
+    uploaded = [torch.cuda.Event() for _ in range(2)]
+    consumed = [torch.cuda.Event() for _ in range(2)]
 
     def e2e_peaks(n_steps):
+        with torch.cuda.stream(copy):
+            d_tpl[0].copy_(h_in, non_blocking=True)
+            uploaded[0].record(copy)
         for s in range(n_steps):
-            templates.copy_(h_in, non_blocking=True)
-            ft.FwdImageInvFFTManyPeaks(ins, images[s % N_IMAGES], peaks)
+            k = s % 2
+            if s + 1 < n_steps:
+                with torch.cuda.stream(copy):
+                    if s >= 1:
+                        copy.wait_event(consumed[1 - k])
+                    d_tpl[1 - k].copy_(h_in, non_blocking=True)
+                    uploaded[1 - k].record(copy)
+            main.wait_event(uploaded[k])
+            ft.FwdImageInvFFTManyPeaks(ins2[k], images[s % N_IMAGES], peaks)
+            consumed[k].record(main)
             h_peaks.copy_(peaks, non_blocking=True)
-
-    e2e_peaks(2)
-    torch.cuda.synchronize()
-    barrier(world, torch)
-    f0.record()
-    e2e_peaks(e2e_steps)
-    f1.record()
-    torch.cuda.synchronize()
-    pk_ms = max_over_ranks(world, f0.elapsed_time(f1), torch, dev)
-    pk_value = world * e2e_steps * B / (pk_ms * 1e-3)
+        main.wait_stream(copy)
 
     # ---- cuFFT pad-then-transform comparator (torch.fft) ----
     cufft = None
@@ -368,6 +442,11 @@ def run_ours(args, world, rank, local):
         cufft_v = reps / (g0.elapsed_time(g1) * 1e-3)
         cufft = {"value": cufft_v, "unit": UNIT, "how": "torch.fft (cuFFT): pad, rfft2, conj-multiply, irfft2, crop",
                  "ours_over_cufft": value / world / cufft_v}
+
+    # ---- uneven batch (rank 0): FP32 and BF16 storage ----
+    uneven = None
+    if rank == 0 and not args.skip_uneven:
+        uneven = [run_uneven(dev, images[0], "float32"), run_uneven(dev, images[0], "bfloat16")]
 
     # ---- CPU baseline (rank 0, one GPU) and accuracy check of one window ----
     cpu = None
@@ -425,6 +504,7 @@ def run_ours(args, world, rank, local):
             "clocks": clk,
             "cufft_pad_then_transform": cufft,
             "accuracy": accuracy,
+            "uneven_batch": uneven,
         }
         print(json.dumps(line), flush=True)
 
@@ -439,6 +519,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-cufft", action="store_true")
+    ap.add_argument("--skip-uneven", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()
