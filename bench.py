@@ -417,6 +417,16 @@ def run_ours(args, world, rank, local):
             h_peaks.copy_(peaks, non_blocking=True)
         main.wait_stream(copy)
 
+    e2e_peaks(2)
+    torch.cuda.synchronize()
+    barrier(world, torch)
+    f0.record()
+    e2e_peaks(e2e_steps)
+    f1.record()
+    torch.cuda.synchronize()
+    pk_ms = max_over_ranks(world, f0.elapsed_time(f1), torch, dev)
+    pk_value = world * e2e_steps * B / (pk_ms * 1e-3)
+
     # ---- cuFFT pad-then-transform comparator (torch.fft) ----
     cufft = None
     if rank == 0 and not args.skip_cufft:

@@ -16,56 +16,9 @@
 #pragma once
 
 #include "kernels_2d.cuh"
+#include "tma.cuh"
 
 namespace ffb {
-
-constexpr int kErrTimeout = 1;
-constexpr long long kWaitLimit = 1ll << 26;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void fence_barrier_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// Bulk global -> shared copy of `bytes` (multiple of 16; both addresses 16-byte aligned),
-// completion counted on `bar`.  No multicast.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
-
-// Polls the barrier phase; returns false if it did not complete within the limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
-    const uint32_t a = smem_addr(bar);
-    for (long long i = 0; i < kWaitLimit; i++) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(a), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
 
 // Shared-memory loads of the staged image column, kept at their point of use (a plain
 // load could be hoisted above the forward transform, holding 16 more complex values live
@@ -105,6 +58,7 @@ struct XcorrColArgs {
     const float2* tw;
     int* err;
     int L_g[kMaxBatch];        // per-template valid rows of uneven batches (0: use L)
+    int tile_rows;             // > 0: output in row tiles [n / R][col][n % R] (R = tile_rows)
 };
 
 // Shared-memory plan of the kernel (bytes), shared by the host launcher.
@@ -147,25 +101,17 @@ xcorr_cols_kernel(XcorrColArgs a) {
     const int j = threadIdx.x - f * T;
     const int lcol = SM::t1_col_elems(a.L);
 
-    if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        fence_barrier_init();
-        uint32_t bytes = (uint32_t)SM::kImgBytes;
-        for (int g = 0; g < a.n_batch; g++) bytes += (uint32_t)SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8;
-        mbar_arrive_expect_tx(bar, bytes);
+    __shared__ int ok_flag;
+    uint32_t bytes = (uint32_t)SM::kImgBytes;
+    for (int g = 0; g < a.n_batch; g++) bytes += (uint32_t)SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8;
+    const bool staged = stage_block(bar, &ok_flag, bytes, a.err, [&]() {
         bulk_g2s(sm_raw + SM::img_off(), static_cast<const ImgC*>(a.img) + (long long)col * a.img_stride,
                  SM::kImgBytes, bar);
         for (int g = 0; g < a.n_batch; g++)
             bulk_g2s(t1_s + g * lcol, a.t1 + g * a.t1_batch + (long long)col * a.t1_pitch,
                      SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8, bar);
-    }
-    __syncthreads();  // barrier initialised before anyone polls it
-    if (!mbar_wait(bar, 0)) {
-        if (threadIdx.x == 0) atomicExch(a.err, kErrTimeout);
-        // give the copies a second bounded chance to land before the block exits
-        mbar_wait(bar, 0);
-        return;
-    }
+    });
+    if (!staged) return;
 
     const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
     const int rounds = (a.n_batch + FPB - 1) / FPB;
@@ -195,11 +141,22 @@ xcorr_cols_kernel(XcorrColArgs a) {
         }
         BlockFft<N, true>::run(v, grp, j, a.tw, 16);
         if (live) {
-            float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
+            if (a.tile_rows > 0) {
+                const int R = a.tile_rows;
+                float2* o = a.out + (long long)g * a.out_batch + (long long)col * R;
+                const long long tile = (long long)a.n_cols * R;
 #pragma unroll
-            for (int q = 0; q < 16; q++) {
-                const int n = j + T * q;
-                if (n < a.W) o[n] = v[q];
+                for (int q = 0; q < 16; q++) {
+                    const int n = j + T * q;
+                    if (n < a.W) o[(n / R) * tile + (n % R)] = v[q];
+                }
+            } else {
+                float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    const int n = j + T * q;
+                    if (n < a.W) o[n] = v[q];
+                }
             }
         }
     }
