@@ -40,6 +40,7 @@ fastfft_status fail(fastfft_plan_s* h, fastfft_status st, const std::string& msg
 }
 
 fastfft_status cuda_fail(fastfft_plan_s* h, cudaError_t e, const char* where) {
+    cudaGetLastError();  // leave no non-sticky error behind for the caller's next CUDA check
     return fail(h, FASTFFT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
@@ -167,9 +168,9 @@ void size_buffers(fastfft_plan_s* h) {
             // templates per launch: bounded by the shared memory of the fused column kernel
             h->red_batch = h->red_batch_request;
             while (h->red_batch > 1 &&
-                   xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, h->red_batch) > 227 * 1024)
+                   xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, h->red_batch) > 226 * 1024)
                 h->red_batch--;
-            if (xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, 1) > 227 * 1024) {
+            if (xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, 1) > 226 * 1024) {
                 h->red_ok = false;
                 h->bytes_c = 0;
                 return;

@@ -33,6 +33,10 @@ cudaError_t twiddles_for(int n, const float2** out);
 // Message returned by fastfft_last_error(NULL), for entry points without a handle.
 void set_unbound_error(const char* msg);
 
+// Raises cudaFuncAttributeMaxDynamicSharedMemorySize of func on the current device to at
+// least `bytes` (per_device: 64 per-device high-water marks owned by the caller).
+cudaError_t ensure_smem_at_least(const void* func, size_t bytes, std::atomic<int>* per_device);
+
 // Sets cudaFuncAttributeMaxDynamicSharedMemorySize once per (kernel, device).
 cudaError_t ensure_smem_attr(const void* func, size_t bytes, std::atomic<unsigned long long>* done_mask);
 

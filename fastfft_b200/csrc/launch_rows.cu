@@ -68,7 +68,7 @@ static cudaError_t c2r_tiles_impl(const RowInvArgs& a, cudaStream_t st) {
     constexpr int FPB = c2r_tile_fpb<N>();
     using SM = C2rTileSmem<N, FPB>;
     constexpr int THREADS = FftShape<N>::T * FPB;
-    if constexpr (SM::kTotal > 227 * 1024) {
+    if constexpr (SM::kTotal > 226 * 1024) {
         return cudaErrorInvalidValue;
     } else {
         static std::atomic<unsigned long long> mask{0};

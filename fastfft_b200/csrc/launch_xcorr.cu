@@ -4,7 +4,8 @@
 
 namespace ffb {
 
-constexpr int kMaxDynSmem = 227 * 1024;
+// dynamic shared memory available to one block (227 KB, less a little static shared memory)
+constexpr int kMaxDynSmem = 227 * 1024 - 1024;
 
 template <int N, class ImgC>
 static cudaError_t xcorr_v2_impl(const XcorrColArgs& a, cudaStream_t st) {
@@ -16,10 +17,10 @@ static cudaError_t xcorr_v2_impl(const XcorrColArgs& a, cudaStream_t st) {
         if (a.n_batch < 1 || a.n_batch > kMaxBatch || a.n_cols < 1) return cudaErrorInvalidValue;
         const int smem = SM::total(a.L, a.n_batch);
         if (smem > kMaxDynSmem) return cudaErrorInvalidValue;
-        static std::atomic<unsigned long long> mask_mul{0}, mask_nomul{0};
+        static std::atomic<int> set_mul[64], set_nomul[64];
         const bool mul = a.intra_kind != 0;
         auto fn = mul ? xcorr_cols_kernel<N, ImgC, FPB, true> : xcorr_cols_kernel<N, ImgC, FPB, false>;
-        cudaError_t e = ensure_smem_attr((const void*)fn, kMaxDynSmem, mul ? &mask_mul : &mask_nomul);
+        cudaError_t e = ensure_smem_at_least((const void*)fn, (size_t)smem, mul ? set_mul : set_nomul);
         if (e != cudaSuccess) return e;
         fn<<<a.n_cols, FftShape<N>::T * FPB, smem, st>>>(a);
         return cudaGetLastError();

@@ -33,6 +33,7 @@ long long ru(long long v, long long m) { return (v + m - 1) / m * m; }
 bool pow2(long long v) { return v >= 1 && (v & (v - 1)) == 0; }
 
 fastfft_status noalloc_fail(fastfft_status st, const std::string& msg) {
+    if (st == FASTFFT_ERR_CUDA) cudaGetLastError();
     set_unbound_error(msg.c_str());
     return st;
 }

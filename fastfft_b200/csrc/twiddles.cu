@@ -80,6 +80,21 @@ cudaError_t twiddles_for(int n, const float2** out) {
     return cudaSuccess;
 }
 
+cudaError_t ensure_smem_at_least(const void* func, size_t bytes, std::atomic<int>* per_device) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::atomic<int>& cur = per_device[dev & 63];
+    if (cur.load(std::memory_order_acquire) >= (int)bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    int prev = cur.load(std::memory_order_relaxed);
+    while (prev < (int)bytes && !cur.compare_exchange_weak(prev, (int)bytes)) {
+    }
+    return cudaSuccess;
+}
+
 cudaError_t ensure_smem_attr(const void* func, size_t bytes, std::atomic<unsigned long long>* done_mask) {
     if (bytes <= 48 * 1024) return cudaSuccess;
     int dev = 0;
