@@ -176,10 +176,7 @@ void size_buffers(fastfft_plan_s* h) {
                 return;
             }
             h->red_t1_stride = round_up((mx / 2 + 1) * h->pitch_a, 32);   // complex elements per template
-            // column output in row tiles of R = c2r_tile_rows(mx) rows: [y / R][kx][y % R]
-            h->red_tile_rows = c2r_tile_rows((int)mx);
-            const long long n_tiles = (h->inv_out.y + h->red_tile_rows - 1) / h->red_tile_rows;
-            h->red_t2_stride = round_up(n_tiles * h->red_tile_rows * (mx / 2 + 1), 32);
+            h->red_t2_stride = round_up((mx / 2 + 1) * h->pitch_b, 32);   // column output [kx][y]
             h->off_c_t1 = h->off_c_spec + round_up(spec, 256);
             h->off_c_t2 = h->off_c_t1 + h->red_batch * h->red_t1_stride * 8;
             h->bytes_c = h->off_c_t2 + h->red_batch * h->red_t2_stride * 8;
@@ -743,7 +740,6 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const
     c.t1 = t1; c.t1_pitch = h->pitch_a; c.t1_batch = h->red_t1_stride; c.L = (int)h->fwd_in.y;
     c.img = spec; c.img_stride = my;
     c.out = t2; c.out_pitch = h->pitch_b; c.out_batch = h->red_t2_stride; c.W = (int)h->inv_out.y;
-    c.tile_rows = h->red_tile_rows;
     c.n_cols = mx / 2 + 1; c.n_batch = n;
     if (dims)
         for (int g = 0; g < n; g++) c.L_g[g] = dims[2 * g + 1];
@@ -759,7 +755,6 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const
     std::memset(&r, 0, sizeof(r));
     r.n_batch = n;
     r.in = t2; r.in_pitch = h->pitch_b; r.in_batch_stride = h->red_t2_stride; r.n_rows = (int)h->inv_out.y;
-    r.err = h->dev_err;
     for (int g = 0; g < n; g++) r.out[g] = outs[g];
     if (peaks) {
         r.peaks = peaks;
@@ -767,7 +762,7 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const
         for (int g = 0; g < n; g++) r.peak_slot[g] = slots[g];
     }
     r.out_pitch = 2LL * h->inv_out.w; r.W = (int)h->inv_out.x; r.scale = scale_of(post_op); r.tw = tw;
-    if ((e = launch_c2r_tiles(mx, h->output_dtype, r, h->stream)) != cudaSuccess)
+    if ((e = launch_c2r_rows(mx, h->output_dtype, r, h->stream)) != cudaSuccess)
         return cuda_fail(h, e, "c2r row pass");
     h->launches++;
     prof_mark(h);

@@ -162,16 +162,6 @@ __device__ __forceinline__ void dft8(float2 (&v)[16]) {
         for (int k2 = 0; k2 < 2; k2++) v[B + S * (k1 + 4 * k2)] = a[2 * k1 + k2];
 }
 
-// DFT8 over v[m + S r], r = 0..7, with m a (fully unrolled) loop index.
-template <bool INV, int S>
-__device__ __forceinline__ void dft8_at(float2 (&v)[16], int m) {
-    if (m == 0) {
-        dft8<INV, 0, S>(v);
-    } else {
-        dft8<INV, 1, S>(v);
-    }
-}
-
 // Twiddle stage inside the 4x4 decomposition of DFT16: a[n1 + 4 k1] *= W16^(n1 k1)
 template <bool INV>
 __device__ __forceinline__ void dft16_inner_twiddles(float2 (&a)[16]) {
@@ -401,7 +391,7 @@ struct BlockFft {
         if constexpr (S::REM > 1) {
             constexpr int R = S::REM;
             constexpr int M = 16 / R;
-            first_pass_pruned<R, M>(v, qnz);
+            first_pass<R, M>(v);
             float2* s = g.begin();
 #pragma unroll
             for (int m = 0; m < M; m++) {
@@ -432,55 +422,6 @@ struct BlockFft {
                 g.sync();
 #pragma unroll
                 for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
-            }
-        }
-    }
-
-    // First pass with zero-padding pruning: butterfly m reads v[m + r M], r < R, and only
-    // the slots below qnz can be non-zero.  One non-zero input: every output equals it.
-    // Two (radix 4 / 8): X[k] = a + b W_R^k.  Otherwise the full DFT.
-    template <int R, int M>
-    __device__ __forceinline__ static void first_pass_pruned(float2 (&v)[16], int qnz) {
-        if (qnz >= 16) {
-            first_pass<R, M>(v);
-            return;
-        }
-#pragma unroll
-        for (int m = 0; m < M; m++) {
-            const int nz = qnz > m ? (qnz - m + M - 1) / M : 0;
-            if (nz <= 1) {
-                const float2 a = v[m];
-#pragma unroll
-                for (int r = 1; r < R; r++) v[m + r * M] = a;
-            } else if (nz == 2 && R == 4) {
-                const float2 a = v[m], b = v[m + M];
-                v[m] = cadd(a, b);
-                v[m + 2 * M] = csub(a, b);
-                if (!INV) {
-                    v[m + M] = make_float2(a.x + b.y, a.y - b.x);
-                    v[m + 3 * M] = make_float2(a.x - b.y, a.y + b.x);
-                } else {
-                    v[m + M] = make_float2(a.x - b.y, a.y + b.x);
-                    v[m + 3 * M] = make_float2(a.x + b.y, a.y - b.x);
-                }
-            } else if (nz == 2 && R == 8) {
-                const float2 a = v[m], b = v[m + M];
-                v[m] = cadd(a, b);
-                v[m + 4 * M] = csub(a, b);
-                v[m + 2 * M] = cadd(a, mul_w16<INV, 4>(b));
-                v[m + 6 * M] = cadd(a, mul_w16<INV, 12>(b));
-                v[m + 1 * M] = cadd(a, mul_w16<INV, 2>(b));
-                v[m + 3 * M] = cadd(a, mul_w16<INV, 6>(b));
-                v[m + 5 * M] = cadd(a, mul_w16<INV, 10>(b));
-                v[m + 7 * M] = cadd(a, mul_w16<INV, 14>(b));
-            } else {
-                if constexpr (R == 2) {
-                    dft2<INV>(v[m], v[m + M]);
-                } else if constexpr (R == 4) {
-                    dft4<INV>(v[m], v[m + M], v[m + 2 * M], v[m + 3 * M]);
-                } else if constexpr (R == 8) {
-                    dft8_at<INV, M>(v, m);
-                }
             }
         }
     }

@@ -283,7 +283,6 @@ struct RowInvArgs {
     unsigned long long* peaks;
     int peaks_only;
     int peak_slot[kMaxBatch];  // batch entry g folds into peaks[peak_slot[g]]
-    int* err;                  // status word of bounded waits (tiled kernel)
 };
 
 // Total order on (value, index) for a 64-bit atomicMax: larger value wins, and among
@@ -349,108 +348,6 @@ c2r_rows_kernel(RowInvArgs a) {
     }
     __syncthreads();
     float2 v[16];
-#pragma unroll
-    for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
-    BlockFft<N, true>::run(v, g, j, a.tw, 16);
-    const int ra = 2 * (blockIdx.x * FPB + f);
-    OutT* oa = static_cast<OutT*>(a.out[blockIdx.y]) + (long long)ra * a.out_pitch;
-    OutT* ob = oa + a.out_pitch;
-    const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
-    if (!a.peaks_only) {
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            const int n = j + T * q - a.X0;
-            if (n >= 0 && n < a.W) {
-                if (has_a) st_real<OutT>(oa + n, v[q].x * a.scale);
-                if (has_b) st_real<OutT>(ob + n, v[q].y * a.scale);
-            }
-        }
-    }
-    if (a.peaks) {
-        unsigned long long best = 0;
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-            const int n = j + T * q - a.X0;
-            if (n >= 0 && n < a.W) {
-                if (has_a) {
-                    const unsigned long long k = peak_key(v[q].x * a.scale, (unsigned)(ra * a.W + n));
-                    best = k > best ? k : best;
-                }
-                if (has_b) {
-                    const unsigned long long k = peak_key(v[q].y * a.scale, (unsigned)((ra + 1) * a.W + n));
-                    best = k > best ? k : best;
-                }
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
-            best = other > best ? other : best;
-        }
-        if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(a.peaks + a.peak_slot[blockIdx.y], best);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Row C2R over row tiles: the input of batch entry g is laid out as
-// [y / R][kx][y % R] (R = 2 * FPB rows per block, kx in [0, N/2]), so one block's whole
-// input is one contiguous tile that a single TMA bulk copy stages into shared memory
-// (the plain kernel gathers N/2+1 strided pieces per block instead).  Output, peak
-// search and scaling as in c2r_rows_kernel.
-// ---------------------------------------------------------------------------
-template <int N, int FPB>
-struct C2rTileSmem {
-    static constexpr int K = N / 2 + 1;
-    static constexpr int R = 2 * FPB;
-    static constexpr int kFftBytes = FftGroup<N, FPB, false>::BYTES;
-    static constexpr int kTileBytes = K * R * 8;
-    static constexpr int kBarOff = (kFftBytes + kTileBytes + 15) & ~15;
-    static constexpr int kTotal = kBarOff + 16;
-};
-
-template <int N, class OutT, int FPB>
-__global__ void __launch_bounds__(FftShape<N>::T * FPB)
-c2r_tiles_kernel(RowInvArgs a) {
-    using S = FftShape<N>;
-    using SM = C2rTileSmem<N, FPB>;
-    using G = FftGroup<N, FPB, false>;
-    constexpr int T = S::T;
-    constexpr int H = N / 2;
-    constexpr int K = SM::K;
-    constexpr int R = SM::R;
-    extern __shared__ __align__(128) unsigned char sm_raw[];
-    float2* smem = reinterpret_cast<float2*>(sm_raw);
-    float2* tile = reinterpret_cast<float2*>(sm_raw + SM::kFftBytes);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm_raw + SM::kBarOff);
-    __shared__ int ok_flag;
-    const int f = threadIdx.x / T;
-    const int j = threadIdx.x - f * T;
-    G g(smem, f);
-    const float2* src = a.in + (long long)blockIdx.y * a.in_batch_stride + (long long)blockIdx.x * (K * R);
-    if (!stage_block(bar, &ok_flag, (uint32_t)SM::kTileBytes, a.err,
-                     [&]() { bulk_g2s(tile, src, SM::kTileBytes, bar); }))
-        return;
-    // Z[k] = A[k] + i B[k] over the full circle for each of the block's FPB row pairs
-    const int items = FPB * K;
-    for (int i = threadIdx.x; i < items; i += T * FPB) {
-        const int ff = i % FPB;
-        const int k = i / FPB;
-        const int rr = 2 * (blockIdx.x * FPB + ff);
-        float2 A = tile[k * R + 2 * ff];
-        float2 B = tile[k * R + 2 * ff + 1];
-        if (rr >= a.n_rows) A = make_float2(0.f, 0.f);
-        if (rr + 1 >= a.n_rows) B = make_float2(0.f, 0.f);
-        float2* sf = smem + ff * G::STRIDE;
-        if (k == 0 || k == H) {
-            sf[phys(k)] = make_float2(A.x, B.x);
-        } else {
-            sf[phys(k)] = make_float2(A.x - B.y, A.y + B.x);
-            sf[phys(N - k)] = make_float2(A.x + B.y, B.x - A.y);
-        }
-    }
-    __syncthreads();
-    float2 v[16];
-    float2* s = g.base;
 #pragma unroll
     for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
     BlockFft<N, true>::run(v, g, j, a.tw, 16);

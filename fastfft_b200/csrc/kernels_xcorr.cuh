@@ -58,7 +58,6 @@ struct XcorrColArgs {
     const float2* tw;
     int* err;
     int L_g[kMaxBatch];        // per-template valid rows of uneven batches (0: use L)
-    int tile_rows;             // > 0: output in row tiles [n / R][col][n % R] (R = tile_rows)
 };
 
 // Shared-memory plan of the kernel (bytes), shared by the host launcher.
@@ -141,22 +140,11 @@ xcorr_cols_kernel(XcorrColArgs a) {
         }
         BlockFft<N, true>::run(v, grp, j, a.tw, 16);
         if (live) {
-            if (a.tile_rows > 0) {
-                const int R = a.tile_rows;
-                float2* o = a.out + (long long)g * a.out_batch + (long long)col * R;
-                const long long tile = (long long)a.n_cols * R;
+            float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const int n = j + T * q;
-                    if (n < a.W) o[(n / R) * tile + (n % R)] = v[q];
-                }
-            } else {
-                float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
-#pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const int n = j + T * q;
-                    if (n < a.W) o[n] = v[q];
-                }
+            for (int q = 0; q < 16; q++) {
+                const int n = j + T * q;
+                if (n < a.W) o[n] = v[q];
             }
         }
     }

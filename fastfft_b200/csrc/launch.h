@@ -17,9 +17,6 @@ struct XcorrColArgs;
 // dtype codes follow fastfft_dtype in include/fastfft_capi.h
 cudaError_t launch_r2c_rows(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
 cudaError_t launch_c2r_rows(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
-// C2R over row tiles [y / R][kx][y % R] staged by one bulk copy per block; R = c2r_tile_rows(n).
-cudaError_t launch_c2r_tiles(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
-int c2r_tile_rows(int n);
 cudaError_t launch_cols_fwd(int n, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st);

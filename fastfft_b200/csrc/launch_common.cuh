@@ -31,12 +31,6 @@ template <int N>
 constexpr int row_fpb() {
     return FftShape<N>::T >= 512 ? 1 : 512 / FftShape<N>::T;
 }
-// Tiled C2R: 256-thread blocks (two FFT groups at N = 2048), so that the staged tile
-// plus the FFT buffers leave room for three blocks per SM.
-template <int N>
-constexpr int c2r_tile_fpb() {
-    return FftShape<N>::T >= 256 ? 1 : 256 / FftShape<N>::T;
-}
 template <int N>
 constexpr int col_fpb() {
     return FftShape<N>::T >= 256 ? 1 : 256 / FftShape<N>::T;

@@ -63,54 +63,5 @@ cudaError_t launch_c2r_rows(int n, int out_dtype, const RowInvArgs& a, cudaStrea
     FFB_SIZE_SWITCH(n, c2r_dispatch, out_dtype, a, st)
 }
 
-template <int N, class OutT>
-static cudaError_t c2r_tiles_impl(const RowInvArgs& a, cudaStream_t st) {
-    constexpr int FPB = c2r_tile_fpb<N>();
-    using SM = C2rTileSmem<N, FPB>;
-    constexpr int THREADS = FftShape<N>::T * FPB;
-    if constexpr (SM::kTotal > 226 * 1024) {
-        return cudaErrorInvalidValue;
-    } else {
-        static std::atomic<unsigned long long> mask{0};
-        auto fn = c2r_tiles_kernel<N, OutT, FPB>;
-        cudaError_t e = ensure_smem_attr((const void*)fn, SM::kTotal, &mask);
-        if (e != cudaSuccess) return e;
-        const int grid = (a.n_rows + SM::R - 1) / SM::R;
-        if (grid == 0) return cudaSuccess;
-        if (a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
-        fn<<<dim3(grid, a.n_batch), THREADS, SM::kTotal, st>>>(a);
-        return cudaGetLastError();
-    }
-}
-
-template <int N>
-static cudaError_t c2r_tiles_dispatch(int out_dtype, const RowInvArgs& a, cudaStream_t st) {
-    switch (out_dtype) {
-        case 0: return c2r_tiles_impl<N, float>(a, st);
-        case 1: return c2r_tiles_impl<N, __half>(a, st);
-        case 2: return c2r_tiles_impl<N, __nv_bfloat16>(a, st);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
-cudaError_t launch_c2r_tiles(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st) {
-    FFB_SIZE_SWITCH(n, c2r_tiles_dispatch, out_dtype, a, st)
-}
-
-int c2r_tile_rows(int n) {
-    switch (n) {
-        case 16: return 2 * c2r_tile_fpb<16>();
-        case 32: return 2 * c2r_tile_fpb<32>();
-        case 64: return 2 * c2r_tile_fpb<64>();
-        case 128: return 2 * c2r_tile_fpb<128>();
-        case 256: return 2 * c2r_tile_fpb<256>();
-        case 512: return 2 * c2r_tile_fpb<512>();
-        case 1024: return 2 * c2r_tile_fpb<1024>();
-        case 2048: return 2 * c2r_tile_fpb<2048>();
-        case 4096: return 2 * c2r_tile_fpb<4096>();
-        case 8192: return 2 * c2r_tile_fpb<8192>();
-        default: return 0;
-    }
-}
 
 }  // namespace ffb

@@ -57,7 +57,6 @@ struct fastfft_plan_s {
     int red_batch = 8;              // templates per launch in the reduced-size path
     int red_batch_request = 8;      // fastfft_set_templates_per_launch (bounded by shared memory)
     long long red_t1_stride = 0, red_t2_stride = 0;  // complex elements per template slice
-    int red_tile_rows = 0;                           // row-tile height of the column output
     long long off_c_t1 = 0, off_c_t2 = 0;
     int* dev_err = nullptr;  // device status word of bounded waits (inside the work buffer)
 

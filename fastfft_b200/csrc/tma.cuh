@@ -1,5 +1,5 @@
 // TMA bulk copies (cp.async.bulk, no multicast) with mbarrier completion and bounded
-// waits, shared by the kernels that stage whole columns or row tiles in shared memory.
+// waits, used by the fused column kernel to stage whole columns in shared memory.
 #pragma once
 
 #include <cuda_runtime.h>
