@@ -19,11 +19,17 @@
 #include <vector>
 
 #include "../../include/fastfft_capi.h"
+#include "fft3.cuh"
 #include "kernels_xcorr.cuh"
 #include "launch.h"
 #include "plan.h"
 
 using namespace ffb;
+
+// Lengths 3 * 2^k for the reduced-size correlation (1), or powers of two only (0).
+#ifndef FFB_ENABLE_FFT3
+#define FFB_ENABLE_FFT3 1
+#endif
 
 namespace {
 
@@ -126,6 +132,17 @@ long long pow2_at_least(long long v) {
     return p;
 }
 
+// Smallest transform length >= v of the reduced-size correlation: a power of two, or
+// 3 * 2^k (kMinP3 <= 2^k <= kMaxP3) when that is shorter.
+long long corr_size_at_least(long long v) {
+    long long best = std::max<long long>(ffb::kMinN, pow2_at_least(v));
+#if FFB_ENABLE_FFT3
+    for (long long p = ffb::kMinP3; p <= ffb::kMaxP3; p *= 2)
+        if (3 * p >= v && 3 * p < best) best = 3 * p;
+#endif
+    return best;
+}
+
 void size_buffers(fastfft_plan_s* h) {
     const long long nx_f = std::max(h->fwd_in.x, h->fwd_out.x);
     const long long kx_f = nx_f / 2 + 1;
@@ -154,8 +171,8 @@ void size_buffers(fastfft_plan_s* h) {
     const bool origin0 = h->org_x == 0 && h->org_y == 0 && h->org_z == 0;
     if (origin0 && h->fwd_change != SizeChange::Decrease && h->inv_change == SizeChange::Decrease) {
         const long long nx = h->fwd_out.x, ny = h->fwd_out.y;
-        const long long mx = std::min(nx, std::max<long long>(ffb::kMinN, pow2_at_least(h->fwd_in.x + h->inv_out.x - 1)));
-        const long long my = std::min(ny, std::max<long long>(ffb::kMinN, pow2_at_least(h->fwd_in.y + h->inv_out.y - 1)));
+        const long long mx = std::min(nx, corr_size_at_least(h->fwd_in.x + h->inv_out.x - 1));
+        const long long my = std::min(ny, corr_size_at_least(h->fwd_in.y + h->inv_out.y - 1));
         if (mx < nx || my < ny) {
             h->red_ok = true;
             h->red_mx = mx;

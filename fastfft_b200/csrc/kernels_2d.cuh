@@ -86,7 +86,8 @@ struct RowFwdArgs {
     long long out_pitch;   // >= n_rows, even
     int kmax;              // kx outputs written (N/2+1, or fewer for a decrease)
     float scale;           // pre-op SCALE (1 = NOOP)
-    const float2* tw;      // twiddle table of size N
+    const float2* tw;      // twiddle table of size N (N = 3P: of the sub-FFT size P)
+    const float2* tw3;     // N = 3P: radix-3 pass twiddles (set by the launcher)
     int n_batch;           // templates in this launch (grid.y)
     // 3D: flat row r = y * rows_z + z reads input row z * rows_y + y, so that the output
     // [kx][y][z] has z contiguous.  rows_z <= 1: row r reads input row r.
@@ -189,6 +190,7 @@ struct ColArgs {
     float in_scale;
     float out_scale;
     const float2* tw;
+    const float2* tw3;       // N = 3P: radix-3 pass twiddles (set by the launcher)
     int n_batch;             // batch entries in this launch (grid.y)
     // General addressing (3D passes); zero values select the plain 2D layout above.
     //   input  column c: (c / in_div) * in_stride + (c % in_div) * in_stride2
@@ -275,6 +277,7 @@ struct RowInvArgs {
     int W;                 // x outputs kept per row: x in [X0, X0 + W)
     float scale;           // post-op SCALE (1 = NOOP)
     const float2* tw;
+    const float2* tw3;     // N = 3P: radix-3 pass twiddles (set by the launcher)
     int n_batch;           // batch entries in this launch (grid.y)
     int X0;
     // Fused peak search: if peaks is set, batch entry g's maximum over the retained

@@ -1,0 +1,327 @@
+// Pass kernels at the lengths N = 3P of the reduced-size correlation (sm_100a).
+//
+// Same argument structures, data layouts and outputs as the power-of-two kernels in
+// kernels_2d.cuh / kernels_xcorr.cuh; only the FFT inside differs (BlockFft3, fft3.cuh):
+//   r2c3_rows_kernel   : row R2C, two real rows per complex FFT, transposed [kx][y] output
+//   c2r3_rows_kernel   : row C2R from [kx][y], two rows per complex FFT, fused peak search
+//   cols3_fwd_kernel   : forward column FFT (2D layout), zero padding y >= L, keep W
+//   xcorr3_cols_kernel : batched fused column pass (TMA-staged image and template columns,
+//                        forward, conj(T) * I, inverse), keep W
+// Time-domain data are loaded and stored in natural order; the spectrum side is decimated
+// by 3 (thread (k2, j) holds X[3 (j + T' q) + k2]).
+#pragma once
+
+#include "fft3.cuh"
+#include "kernels_xcorr.cuh"
+
+namespace ffb {
+
+// ---------------------------------------------------------------------------
+// Row R2C (forward)
+// ---------------------------------------------------------------------------
+#ifndef FFB_ROWS3_MIN_BLOCKS
+#define FFB_ROWS3_MIN_BLOCKS 2
+#endif
+
+template <int P, class InT, int FPB>
+__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, FFB_ROWS3_MIN_BLOCKS)
+r2c3_rows_kernel(RowFwdArgs a) {
+    using S3 = Fft3Shape<P>;
+    constexpr int N = S3::N;
+    constexpr int T = S3::T;
+    constexpr int TP = S3::TP;
+    extern __shared__ float2 smem[];
+    using G = Fft3Group<P, FPB, false>;
+    const int f = threadIdx.x / T;
+    const int t = threadIdx.x - f * T;
+    const int k2 = t / TP;
+    const int j = t - k2 * TP;
+    G g(smem, f, k2);
+    const int gb = blockIdx.y;
+    const int n_rows = a.rows_g[gb] > 0 ? a.rows_g[gb] : a.n_rows;
+    const int L = a.L_g[gb] > 0 ? a.L_g[gb] : a.L;
+    const long long in_pitch = a.pitch_g[gb] > 0 ? a.pitch_g[gb] : a.in_pitch;
+    const int ra = 2 * (blockIdx.x * FPB + f);
+    const bool has_a = ra < n_rows, has_b = ra + 1 < n_rows;
+    const InT* in_g = static_cast<const InT*>(a.in[gb]);
+    const InT* pa = in_g + input_row(ra, a.rows_y, a.rows_z) * in_pitch;
+    const InT* pb = in_g + input_row(ra + 1, a.rows_y, a.rows_z) * in_pitch;
+    float2* const out_g = a.out + (long long)blockIdx.y * a.out_batch_stride;
+    // two real rows as one complex sequence z[n] = a[n] + i b[n]; thread (r, j) holds
+    // z[3 (j + T' q) + r] (decimation in time: the sub-FFTs share the row's samples)
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int n = 3 * (j + TP * q) + k2;
+        float xa = 0.f, xb = 0.f;
+        if (n < L) {
+            if (has_a) xa = ld_real<InT>(pa + n);
+            if (has_b) xb = ld_real<InT>(pb + n);
+        }
+        v[q] = make_float2(xa * a.scale, xb * a.scale);
+    }
+    forward_dit<P>(v, g, j, t, a.tw, a.tw3, leading_slots_dit<P>(L, k2, j));
+
+    // Split Z = A + iB into the two real-row spectra (every FFT's buffer is read by the
+    // whole block): A[k] = (Z[k] + conj Z[N-k]) / 2, B[k] = -i (Z[k] - conj Z[N-k]) / 2.
+    __syncthreads();
+    const int items = FPB * a.kmax;
+    constexpr int kItemsPerThread = (FPB * (N / 2 + 1) + T * FPB - 1) / (T * FPB);
+#pragma unroll
+    for (int it = 0; it < kItemsPerThread; it++) {
+        const int i = threadIdx.x + it * (T * FPB);
+        if (i >= items) continue;
+        const int ff = i % FPB;
+        const int k = i / FPB;
+        const float2* sf = smem + ff * G::STRIDE;
+        const float2 z1 = sf[loc3<P>(k)];
+        const float2 z2 = sf[loc3<P>(k == 0 ? 0 : N - k)];
+        const float2 A = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
+        const float2 B = make_float2(0.5f * (z1.y + z2.y), 0.5f * (z2.x - z1.x));
+        const int rr = 2 * (blockIdx.x * FPB + ff);
+        float2* o = out_g + (long long)k * a.out_pitch + rr;
+        if (rr + 1 < n_rows) {
+            *reinterpret_cast<float4*>(o) = make_float4(A.x, A.y, B.x, B.y);
+        } else if (rr < n_rows) {
+            *o = A;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row C2R (inverse), optional fused peak search
+// ---------------------------------------------------------------------------
+template <int P, class OutT, int FPB>
+__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, FFB_ROWS3_MIN_BLOCKS)
+c2r3_rows_kernel(RowInvArgs a) {
+    using S3 = Fft3Shape<P>;
+    constexpr int N = S3::N;
+    constexpr int T = S3::T;
+    constexpr int TP = S3::TP;
+    constexpr int H = N / 2;
+    extern __shared__ float2 smem[];
+    using G = Fft3Group<P, FPB, false>;
+    const int f = threadIdx.x / T;
+    const int t = threadIdx.x - f * T;
+    const int k2 = t / TP;
+    const int j = t - k2 * TP;
+    G g(smem, f, k2);
+    // Gather rows (2 per FFT) and build Z[k] = A[k] + i B[k] over the full circle from the
+    // half spectra; the imaginary parts of the k = 0 and k = N/2 bins are dropped.
+    const int items = FPB * (H + 1);
+    constexpr int kItemsPerThread = (FPB * (H + 1) + T * FPB - 1) / (T * FPB);
+    float4 ld[kItemsPerThread];
+#pragma unroll
+    for (int it = 0; it < kItemsPerThread; it++) {
+        const int i = threadIdx.x + it * (T * FPB);
+        const int ff = i % FPB;
+        const int k = i / FPB;
+        const int rr = 2 * (blockIdx.x * FPB + ff);
+        const float2* p = a.in + (long long)blockIdx.y * a.in_batch_stride + (long long)k * a.in_pitch + rr;
+        ld[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (i < items) {
+            if (rr + 1 < a.n_rows) {
+                ld[it] = *reinterpret_cast<const float4*>(p);
+            } else if (rr < a.n_rows) {
+                const float2 x = *p;
+                ld[it] = make_float4(x.x, x.y, 0.f, 0.f);
+            }
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < kItemsPerThread; it++) {
+        const int i = threadIdx.x + it * (T * FPB);
+        if (i < items) {
+            const int ff = i % FPB;
+            const int k = i / FPB;
+            const float2 A = make_float2(ld[it].x, ld[it].y), B = make_float2(ld[it].z, ld[it].w);
+            float2* sf = smem + ff * G::STRIDE;
+            if (k == 0 || k == H) {
+                sf[loc3<P>(k)] = make_float2(A.x, B.x);
+            } else {
+                sf[loc3<P>(k)] = make_float2(A.x - B.y, A.y + B.x);
+                sf[loc3<P>(N - k)] = make_float2(A.x + B.y, B.x - A.y);
+            }
+        }
+    }
+    __syncthreads();
+    float2 v[16];
+    {
+        const float2* z = g.base;
+#pragma unroll
+        for (int q = 0; q < 16; q++) v[q] = z[loc3<P>(3 * (j + TP * q) + k2)];
+    }
+    g.sync_fft();  // the reads above cross regions; the sub-FFT exchanges rewrite them
+    BlockFft<P, true>::run(v, g, j, a.tw, 16);
+    const int ra = 2 * (blockIdx.x * FPB + f);
+    OutT* oa = static_cast<OutT*>(a.out[blockIdx.y]) + (long long)ra * a.out_pitch;
+    OutT* ob = oa + a.out_pitch;
+    const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
+    const bool write = !a.peaks_only;
+    unsigned long long best = 0;
+    dit_output<P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
+        const int n = n0 - a.X0;
+        if (n >= 0 && n < a.W) {
+            const float va = x.x * a.scale, vb = x.y * a.scale;
+            if (write) {
+                if (has_a) st_real<OutT>(oa + n, va);
+                if (has_b) st_real<OutT>(ob + n, vb);
+            }
+            if (a.peaks) {
+                if (has_a) {
+                    const unsigned long long k = peak_key(va, (unsigned)(ra * a.W + n));
+                    best = k > best ? k : best;
+                }
+                if (has_b) {
+                    const unsigned long long k = peak_key(vb, (unsigned)((ra + 1) * a.W + n));
+                    best = k > best ? k : best;
+                }
+            }
+        }
+    });
+    if (a.peaks) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+            best = other > best ? other : best;
+        }
+        if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(a.peaks + a.peak_slot[blockIdx.y], best);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Forward column FFT over the 2D [kx][y] layout (the image preparation of the
+// reduced-size correlation); general 3D addressing is not supported at these lengths.
+// ---------------------------------------------------------------------------
+template <int P, int FPB>
+__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB)
+cols3_fwd_kernel(ColArgs a) {
+    using S3 = Fft3Shape<P>;
+    constexpr int T = S3::T;
+    constexpr int TP = S3::TP;
+    extern __shared__ float2 smem[];
+    using G = Fft3Group<P, FPB, true>;
+    const int f = threadIdx.x / T;
+    const int t = threadIdx.x - f * T;
+    const int k2 = t / TP;
+    const int j = t - k2 * TP;
+    G g(smem, f, k2);
+    const int col = blockIdx.x * FPB + f;
+    const bool valid = col < a.n_cols;
+    const long long bz = blockIdx.y;
+    const float2* pin = static_cast<const float2*>(a.in) + bz * a.in_batch_stride + (long long)col * a.in_stride;
+    auto ld = [&](int n) {
+        const float2 x = (valid && n < a.L) ? pin[n] : make_float2(0.f, 0.f);
+        return (a.in_scale != 1.f) ? cscale(x, a.in_scale) : x;
+    };
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int n1 = j + TP * q;
+        v[q] = dif_input<P>(ld(n1), ld(n1 + P), ld(n1 + 2 * P), n1, k2, a.tw3);
+    }
+    BlockFft<P, false>::run(v, g, j, a.tw, valid ? leading_slots3<P>(a.L, j) : 0);
+    if (valid) {
+        float2* pout = static_cast<float2*>(a.out) + bz * a.out_batch_stride + (long long)col * a.out_stride;
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int k = 3 * (j + TP * q) + k2;
+            if (k < a.W) pout[k] = (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batched fused correlation column pass (as xcorr_cols_kernel)
+// ---------------------------------------------------------------------------
+template <int P, class ImgC, int FPB>
+struct Xcorr3Smem {
+    static constexpr int kImgBytes = 3 * P * (int)sizeof(ImgC);
+    static constexpr int kXchBytes = Fft3Group<P, FPB, true>::BYTES;
+    static __host__ __device__ constexpr int t1_col_elems(int L) { return (L + 1) & ~1; }  // 16-byte multiple
+    static __host__ __device__ constexpr int img_off() { return 0; }
+    static __host__ __device__ constexpr int xch_off() { return (kImgBytes + 127) & ~127; }
+    static __host__ __device__ constexpr int t1_off() { return xch_off() + kXchBytes; }
+    static __host__ __device__ constexpr int bar_off(int L, int nb) {
+        return (t1_off() + nb * t1_col_elems(L) * 8 + 15) & ~15;
+    }
+    static __host__ __device__ constexpr int total(int L, int nb) { return bar_off(L, nb) + 16; }
+};
+
+#ifndef FFB_XCORR3_MIN_BLOCKS
+#define FFB_XCORR3_MIN_BLOCKS 2
+#endif
+
+template <int P, class ImgC, int FPB, bool MUL>
+__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, (Fft3Shape<P>::T * FPB <= 256) ? FFB_XCORR3_MIN_BLOCKS : 1)
+xcorr3_cols_kernel(XcorrColArgs a) {
+    using S3 = Fft3Shape<P>;
+    using SM = Xcorr3Smem<P, ImgC, FPB>;
+    constexpr int T = S3::T;
+    constexpr int TP = S3::TP;
+    extern __shared__ __align__(128) unsigned char sm_raw[];
+    const ImgC* img_s = reinterpret_cast<const ImgC*>(sm_raw + SM::img_off());
+    float2* xch = reinterpret_cast<float2*>(sm_raw + SM::xch_off());
+    float2* t1_s = reinterpret_cast<float2*>(sm_raw + SM::t1_off());
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm_raw + SM::bar_off(a.L, a.n_batch));
+
+    const int col = blockIdx.x;
+    const int f = threadIdx.x / T;
+    const int t = threadIdx.x - f * T;
+    const int k2 = t / TP;
+    const int j = t - k2 * TP;
+    const int lcol = SM::t1_col_elems(a.L);
+
+    __shared__ int ok_flag;
+    uint32_t bytes = (uint32_t)SM::kImgBytes;
+    for (int g = 0; g < a.n_batch; g++) bytes += (uint32_t)SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8;
+    const bool staged = stage_block(bar, &ok_flag, bytes, a.err, [&]() {
+        bulk_g2s(sm_raw + SM::img_off(), static_cast<const ImgC*>(a.img) + (long long)col * a.img_stride,
+                 SM::kImgBytes, bar);
+        for (int g = 0; g < a.n_batch; g++)
+            bulk_g2s(t1_s + g * lcol, a.t1 + g * a.t1_batch + (long long)col * a.t1_pitch,
+                     SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8, bar);
+    });
+    if (!staged) return;
+
+    const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
+    const int rounds = (a.n_batch + FPB - 1) / FPB;
+    Fft3Group<P, FPB, true> grp(xch, f, k2);
+#pragma unroll 1
+    for (int it = 0; it < rounds; it++) {
+        const int g = it * FPB + f;
+        const bool live = g < a.n_batch;
+        const int Lg = (live && a.L_g[g] > 0) ? a.L_g[g] : a.L;
+        // keep the next template's loads out of this template's transforms
+        asm volatile("" ::: "memory");
+        // the previous round's output pass read all three regions of one buffer, which the
+        // sub-FFT exchanges below rewrite
+        if (it > 0) grp.sync_fft();
+        float2 v[16];
+        const float2* src = t1_s + (live ? g : 0) * lcol;
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int n1 = j + TP * q;
+            const float2 x0 = (live && n1 < Lg) ? src[n1] : make_float2(0.f, 0.f);
+            const float2 x1 = (live && n1 + P < Lg) ? src[n1 + P] : make_float2(0.f, 0.f);
+            const float2 x2 = (live && n1 + 2 * P < Lg) ? src[n1 + 2 * P] : make_float2(0.f, 0.f);
+            v[q] = dif_input<P>(x0, x1, x2, n1, k2, a.tw3);
+        }
+        BlockFft<P, false>::run(v, grp, j, a.tw, live ? leading_slots3<P>(Lg, j) : 0);
+        if constexpr (MUL) {
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const float2 im = lds_cplx<ImgC>(img_s + 3 * (j + TP * q) + k2);
+                v[q] = cscale(conj_mul(v[q], im), sc);
+            }
+        }
+        BlockFft<P, true>::run(v, grp, j, a.tw, 16);
+        float2* o = a.out + (long long)(live ? g : 0) * a.out_batch + (long long)col * a.out_pitch;
+        const int W = live ? a.W : 0;
+        dit_output<P>(v, grp, j, t, a.tw3, [&](int n, float2 x) {
+            if (n < W) o[n] = x;
+        });
+    }
+}
+
+}  // namespace ffb

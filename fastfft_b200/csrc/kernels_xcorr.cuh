@@ -56,6 +56,7 @@ struct XcorrColArgs {
     int intra_kind;            // 0 NOOP, 2 CONJ_MUL, 3 CONJ_MUL_THEN_SCALE
     float intra_scale;
     const float2* tw;
+    const float2* tw3;         // N = 3P: radix-3 pass twiddles (set by the launcher)
     int* err;
     int L_g[kMaxBatch];        // per-template valid rows of uneven batches (0: use L)
 };

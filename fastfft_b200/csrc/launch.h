@@ -1,6 +1,7 @@
 // Host-side launchers for the pass kernels (one translation unit per kernel family,
 // so the sm_100a build compiles in parallel).  Each launcher picks the compile-time
-// FFT size from the runtime N (power of two in [16, 8192]) and the data types.
+// FFT size from the runtime N (power of two in [16, 8192], or 3P for the passes of the
+// reduced-size correlation) and the data types.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -24,7 +25,16 @@ cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream
 cudaError_t launch_xcorr_cols(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st);
 size_t xcorr_cols_smem(int n, int img_dtype, int L, int n_batch);
 
-// Device-wide FP64-generated twiddle table (generated once per device).
+// Lengths N = 3P (128 <= P <= 2048) of the reduced-size correlation; the public
+// launchers above forward them here (R2C, C2R, forward columns, fused columns only).
+cudaError_t launch_r2c3(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
+cudaError_t launch_c2r3(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
+cudaError_t launch_cols3_fwd(int n, const ColArgs& a, cudaStream_t st);
+cudaError_t launch_xcorr3(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st);
+size_t xcorr3_smem(int n, int img_dtype, int L, int n_batch);
+
+// Device-wide FP64-generated twiddle tables (generated once per device): for a power of
+// two n the radix-16 pass table, for n = 3P the radix-3 pass table W_n^m, m < 2P.
 cudaError_t twiddles_for(int n, const float2** out);
 
 // Message returned by fastfft_last_error(NULL), for entry points without a handle.

@@ -42,7 +42,10 @@ static cudaError_t xcorr_dispatch(int img_dtype, const ColArgs& a, cudaStream_t 
     }
 }
 
-cudaError_t launch_cols_fwd(int n, const ColArgs& a, cudaStream_t st) { FFB_SIZE_SWITCH(n, fwd_dispatch, a, st) }
+cudaError_t launch_cols_fwd(int n, const ColArgs& a, cudaStream_t st) {
+    if (is_3p_size(n)) return launch_cols3_fwd(n, a, st);
+    FFB_SIZE_SWITCH(n, fwd_dispatch, a, st)
+}
 cudaError_t launch_cols_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st) {
     FFB_SIZE_SWITCH(n, inv_dispatch, in_dtype, a, st)
 }

@@ -3,6 +3,7 @@
 
 #include <atomic>
 
+#include "fft3.cuh"
 #include "kernels_2d.cuh"
 #include "launch.h"
 

@@ -1,0 +1,187 @@
+// Launchers for the length-3P pass kernels (kernels_fft3.cuh).  The public launchers in
+// launch_rows.cu / launch_cols.cu / launch_xcorr.cu forward N = 3P here; the caller's
+// `tw` is replaced by the two tables these kernels read (sub-FFT size P, radix-3 pass).
+#include "kernels_fft3.cuh"
+#include "launch_common.cuh"
+
+namespace ffb {
+
+#define FFB_SIZE3_SWITCH(n, FN, ...)                 \
+    switch (n) {                                     \
+        case 3 * 128: return FN<128>(__VA_ARGS__);   \
+        case 3 * 256: return FN<256>(__VA_ARGS__);   \
+        case 3 * 512: return FN<512>(__VA_ARGS__);   \
+        case 3 * 1024: return FN<1024>(__VA_ARGS__); \
+        case 3 * 2048: return FN<2048>(__VA_ARGS__); \
+        default: return cudaErrorInvalidValue;       \
+    }
+
+// FFTs per block: up to about 512 threads for the row passes and 256 for the column
+// passes, in whole warps (the peak search shuffles over full warps)
+constexpr int fpb3_for(int t, int target) {
+    int f = target / t;
+    if (f < 1) f = 1;
+    while (f > 1 && (t * f) % 32 != 0) f--;
+    return f;
+}
+template <int P>
+constexpr int row_fpb3() {
+    return fpb3_for(Fft3Shape<P>::T, 512);
+}
+template <int P>
+constexpr int col_fpb3() {
+    return fpb3_for(Fft3Shape<P>::T, 256);
+}
+static_assert(Fft3Shape<128>::T * row_fpb3<128>() % 32 == 0 && Fft3Shape<128>::T * col_fpb3<128>() % 32 == 0, "warps");
+static_assert(Fft3Shape<256>::T * row_fpb3<256>() % 32 == 0 && Fft3Shape<256>::T * col_fpb3<256>() % 32 == 0, "warps");
+
+static cudaError_t tables3(int p, const float2** tw, const float2** tw3) {
+    cudaError_t e = twiddles_for(p, tw);
+    if (e != cudaSuccess) return e;
+    return twiddles_for(3 * p, tw3);
+}
+
+// ---------------------------------------------------------------------------
+template <int P, class InT>
+static cudaError_t r2c3_impl(const RowFwdArgs& a0, cudaStream_t st) {
+    constexpr int FPB = row_fpb3<P>();
+    constexpr int THREADS = Fft3Shape<P>::T * FPB;
+    const size_t smem = (size_t)Fft3Group<P, FPB, false>::BYTES;
+    RowFwdArgs a = a0;
+    cudaError_t e = tables3(P, &a.tw, &a.tw3);
+    if (e != cudaSuccess) return e;
+    static std::atomic<unsigned long long> mask{0};
+    auto fn = r2c3_rows_kernel<P, InT, FPB>;
+    if ((e = ensure_smem_attr((const void*)fn, smem, &mask)) != cudaSuccess) return e;
+    const int grid = (a.n_rows + 2 * FPB - 1) / (2 * FPB);
+    if (grid == 0) return cudaSuccess;
+    if (a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
+    fn<<<dim3(grid, a.n_batch), THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P>
+static cudaError_t r2c3_dispatch(int in_dtype, const RowFwdArgs& a, cudaStream_t st) {
+    switch (in_dtype) {
+        case 0: return r2c3_impl<P, float>(a, st);
+        case 1: return r2c3_impl<P, __half>(a, st);
+        case 2: return r2c3_impl<P, __nv_bfloat16>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_r2c3(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st) {
+    FFB_SIZE3_SWITCH(n, r2c3_dispatch, in_dtype, a, st)
+}
+
+// ---------------------------------------------------------------------------
+template <int P, class OutT>
+static cudaError_t c2r3_impl(const RowInvArgs& a0, cudaStream_t st) {
+    constexpr int FPB = row_fpb3<P>();
+    constexpr int THREADS = Fft3Shape<P>::T * FPB;
+    const size_t smem = (size_t)Fft3Group<P, FPB, false>::BYTES;
+    RowInvArgs a = a0;
+    cudaError_t e = tables3(P, &a.tw, &a.tw3);
+    if (e != cudaSuccess) return e;
+    static std::atomic<unsigned long long> mask{0};
+    auto fn = c2r3_rows_kernel<P, OutT, FPB>;
+    if ((e = ensure_smem_attr((const void*)fn, smem, &mask)) != cudaSuccess) return e;
+    const int grid = (a.n_rows + 2 * FPB - 1) / (2 * FPB);
+    if (grid == 0) return cudaSuccess;
+    if (a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
+    fn<<<dim3(grid, a.n_batch), THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P>
+static cudaError_t c2r3_dispatch(int out_dtype, const RowInvArgs& a, cudaStream_t st) {
+    switch (out_dtype) {
+        case 0: return c2r3_impl<P, float>(a, st);
+        case 1: return c2r3_impl<P, __half>(a, st);
+        case 2: return c2r3_impl<P, __nv_bfloat16>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_c2r3(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st) {
+    FFB_SIZE3_SWITCH(n, c2r3_dispatch, out_dtype, a, st)
+}
+
+// ---------------------------------------------------------------------------
+template <int P>
+static cudaError_t cols3_fwd_impl(const ColArgs& a0, cudaStream_t st) {
+    // 2D layout only (the image preparation of the reduced-size correlation)
+    if (a0.in_div > 1 || a0.out_div > 1 || a0.out_elem_stride > 1 || a0.W0 != 0) return cudaErrorInvalidValue;
+    constexpr int FPB = col_fpb3<P>();
+    constexpr int THREADS = Fft3Shape<P>::T * FPB;
+    const size_t smem = (size_t)Fft3Group<P, FPB, true>::BYTES;
+    ColArgs a = a0;
+    cudaError_t e = tables3(P, &a.tw, &a.tw3);
+    if (e != cudaSuccess) return e;
+    static std::atomic<unsigned long long> mask{0};
+    auto fn = cols3_fwd_kernel<P, FPB>;
+    if ((e = ensure_smem_attr((const void*)fn, smem, &mask)) != cudaSuccess) return e;
+    const int grid = (a.n_cols + FPB - 1) / FPB;
+    if (grid == 0) return cudaSuccess;
+    if (a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
+    fn<<<dim3(grid, a.n_batch), THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cols3_fwd(int n, const ColArgs& a, cudaStream_t st) { FFB_SIZE3_SWITCH(n, cols3_fwd_impl, a, st) }
+
+// ---------------------------------------------------------------------------
+// dynamic shared memory available to one block (227 KB, less a little static shared memory)
+constexpr int kMaxDynSmem3 = 227 * 1024 - 1024;
+
+template <int P, class ImgC>
+static cudaError_t xcorr3_impl(const XcorrColArgs& a0, cudaStream_t st) {
+    constexpr int FPB = col_fpb3<P>();
+    using SM = Xcorr3Smem<P, ImgC, FPB>;
+    if (a0.n_batch < 1 || a0.n_batch > kMaxBatch || a0.n_cols < 1) return cudaErrorInvalidValue;
+    const int smem = SM::total(a0.L, a0.n_batch);
+    if (smem > kMaxDynSmem3) return cudaErrorInvalidValue;
+    XcorrColArgs a = a0;
+    cudaError_t e = tables3(P, &a.tw, &a.tw3);
+    if (e != cudaSuccess) return e;
+    static std::atomic<int> set_mul[64], set_nomul[64];
+    const bool mul = a.intra_kind != 0;
+    auto fn = mul ? xcorr3_cols_kernel<P, ImgC, FPB, true> : xcorr3_cols_kernel<P, ImgC, FPB, false>;
+    if ((e = ensure_smem_at_least((const void*)fn, (size_t)smem, mul ? set_mul : set_nomul)) != cudaSuccess) return e;
+    fn<<<a.n_cols, Fft3Shape<P>::T * FPB, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P>
+static cudaError_t xcorr3_dispatch(int img_dtype, const XcorrColArgs& a, cudaStream_t st) {
+    switch (img_dtype) {
+        case 3: return xcorr3_impl<P, float2>(a, st);
+        case 4: return xcorr3_impl<P, __half2>(a, st);
+        case 5: return xcorr3_impl<P, __nv_bfloat162>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_xcorr3(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st) {
+    FFB_SIZE3_SWITCH(n, xcorr3_dispatch, img_dtype, a, st)
+}
+
+template <int P>
+static size_t xcorr3_smem_p(int img_dtype, int L, int n_batch) {
+    constexpr int FPB = col_fpb3<P>();
+    if (img_dtype == 3) return (size_t)Xcorr3Smem<P, float2, FPB>::total(L, n_batch);
+    return (size_t)Xcorr3Smem<P, __half2, FPB>::total(L, n_batch);
+}
+
+size_t xcorr3_smem(int n, int img_dtype, int L, int n_batch) {
+    switch (n) {
+        case 3 * 128: return xcorr3_smem_p<128>(img_dtype, L, n_batch);
+        case 3 * 256: return xcorr3_smem_p<256>(img_dtype, L, n_batch);
+        case 3 * 512: return xcorr3_smem_p<512>(img_dtype, L, n_batch);
+        case 3 * 1024: return xcorr3_smem_p<1024>(img_dtype, L, n_batch);
+        case 3 * 2048: return xcorr3_smem_p<2048>(img_dtype, L, n_batch);
+        default: return ~(size_t)0;
+    }
+}
+
+}  // namespace ffb

@@ -43,14 +43,34 @@ static __global__ void init_twiddles_kernel(float2* tw) {
 }
 
 
+// Radix-3 pass tables of the lengths N = 3P: W_N^m = exp(-2 pi i m / N), m < 2P.
+static __global__ void init_twiddles3_kernel(float2* tw) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= kTw3Total) return;
+    for (int p = kMinP3; p <= kMaxP3; p *= 2) {
+        const int base = tw3_base(p);
+        if (gid < base + tw3_size_of(p)) {
+            const int m = gid - base;
+            // exp(-2 pi i m / 3p) = cospi(-x) + i sinpi(-x), x = 2 m / 3p
+            const double x = -2.0 * (double)m / (3.0 * (double)p);
+            double sv, cv;
+            sincospi(x, &sv, &cv);
+            tw[gid] = make_float2((float)cv, (float)sv);
+            return;
+        }
+    }
+}
+
 // One table for every supported size, generated on the device in FP64 and rounded
 // once to FP32 (the reference evaluates __sincosf per element instead,
 // include/detail/device_functions.h:17-27).
 __device__ float2 g_twiddles[kTwTotal];
+__device__ float2 g_twiddles3[kTw3Total];
 
 namespace {
 std::mutex g_tw_mutex;
 const float2* g_tw_ptr[64] = {nullptr};
+const float2* g_tw3_ptr[64] = {nullptr};
 }  // namespace
 
 cudaError_t twiddles_for(int n, const float2** out) {
@@ -61,19 +81,32 @@ cudaError_t twiddles_for(int n, const float2** out) {
     std::lock_guard<std::mutex> lock(g_tw_mutex);
     if (!g_tw_ptr[dev]) {
         void* p = nullptr;
+        void* p3 = nullptr;
         e = cudaGetSymbolAddress(&p, g_twiddles);
+        if (e != cudaSuccess) return e;
+        e = cudaGetSymbolAddress(&p3, g_twiddles3);
         if (e != cudaSuccess) return e;
         cudaStream_t s;
         e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
         if (e != cudaSuccess) return e;
         init_twiddles_kernel<<<(kTwTotal + 255) / 256, 256, 0, s>>>(static_cast<float2*>(p));
         e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            init_twiddles3_kernel<<<(kTw3Total + 255) / 256, 256, 0, s>>>(static_cast<float2*>(p3));
+            e = cudaGetLastError();
+        }
         cudaError_t e2 = cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
         if (e != cudaSuccess) return e;
         if (e2 != cudaSuccess) return e2;
         g_tw_ptr[dev] = static_cast<const float2*>(p);
+        g_tw3_ptr[dev] = static_cast<const float2*>(p3);
     }
+    if (is_3p_size(n)) {
+        *out = g_tw3_ptr[dev] + tw3_base(n / 3);
+        return cudaSuccess;
+    }
+    if (!is_pow2_size(n) || n < kMinN || n > kMaxN) return cudaErrorInvalidValue;
     int base = 0;
     for (int m = kMinN; m < n; m *= 2) base += tw_size_of(m);
     *out = g_tw_ptr[dev] + base;

@@ -95,7 +95,7 @@ class FourierTransformer:
                 lib.fastfft_destroy(h)
             except Exception:  # interpreter shutdown: the library may already be gone
                 pass
-            self._h = C.Handle()
+            self._h = None     # (module globals such as C.Handle may be gone at shutdown)
 
     # -- helpers ---------------------------------------------------------
     def _check(self, st):

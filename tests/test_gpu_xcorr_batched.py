@@ -1,7 +1,7 @@
 """Batched correlation (fastfft_fwd_image_inv_many) against the FP64 oracle.
 
-The batched call correlates at the smallest exact size M = pow2 >= L + W - 1 per axis
-when M < N; these tests check that the retained window equals the size-N correlation
+The batched call correlates at the smallest exact size M >= L + W - 1 per axis (a power
+of two or 3 * 2^k) when M < N; these tests check that the retained window equals the size-N correlation
 the reference defines (FwdImageInvFFT, conj(T) * I, origin-anchored crop).
 """
 import numpy as np
@@ -29,9 +29,10 @@ def image_spectrum(fout, seed):
 CASES = [
     ((48, 48, 1), (512, 512, 1), (40, 40, 1), (128, 128)),
     ((100, 60, 1), (1024, 512, 1), (130, 70, 1), (256, 256)),
-    ((128, 128, 1), (4096, 4096, 1), (512, 512, 1), (1024, 1024)),
-    ((256, 256, 1), (1024, 1024, 1), (512, 512, 1), (1024, 1024)),   # M = N: full size
-    ((33, 200, 1), (64, 2048, 1), (30, 100, 1), (64, 512)),
+    ((128, 128, 1), (4096, 4096, 1), (512, 512, 1), (768, 768)),
+    ((256, 256, 1), (1024, 1024, 1), (512, 512, 1), (768, 768)),
+    ((256, 256, 1), (512, 512, 1), (300, 300, 1), (512, 512)),       # 555 > 512: full size
+    ((33, 200, 1), (64, 2048, 1), (30, 100, 1), (64, 384)),
 ]
 
 
@@ -64,7 +65,7 @@ def test_many_equals_full_size_path(torch_cuda):
     a = plan(fin, fout, iout)
     b = plan(fin, fout, iout)
     b.SetFullSizeCorrelation(True)
-    assert a.CorrelationSize() == (512, 512) and b.CorrelationSize() == (1024, 1024)
+    assert a.CorrelationSize() == (384, 384) and b.CorrelationSize() == (1024, 1024)
     oa, ob, oc = (empty(torch, a.ReturnInvOutputMemorySize(), torch.float32) for _ in range(3))
     a.FwdImageInvFFTMany([t], spec, [oa])
     b.FwdImageInvFFTMany([t], spec, [ob])
@@ -75,14 +76,14 @@ def test_many_equals_full_size_path(torch_cuda):
 
 
 def test_many_headline_shape_peak(torch_cuda):
-    """384^2 template, 4096^2 image (noise + blobs), 1024^2 window: computed at 2048^2."""
+    """384^2 template, 4096^2 image (noise + blobs), 1024^2 window: computed at 1536^2."""
     torch = torch_cuda
     n, L, W = 4096, 384, 1024
     spec = O.image_spectrum_fp32(O.gaussian_blob_image(n))
     t = O.normal_template(L, O.SEED_BASE + 1).astype(np.float32)
     fin, fout, iout = (L, L, 1), (n, n, 1), (W, W, 1)
     ft = plan(fin, fout, iout)
-    assert ft.CorrelationSize() == (2048, 2048)
+    assert ft.CorrelationSize() == (1536, 1536)
     out = empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32)
     ft.FwdImageInvFFTMany([dev(torch, O.real_to_padded(t, fin))], dev(torch, spec.view(np.float32)), [out])
     got = O.real_from_padded(host(out), iout)[0]
