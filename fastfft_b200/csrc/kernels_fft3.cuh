@@ -234,10 +234,16 @@ cols3_fwd_kernel(ColArgs a) {
 // ---------------------------------------------------------------------------
 // Batched fused correlation column pass (as xcorr_cols_kernel)
 // ---------------------------------------------------------------------------
+// One exchange buffer per FFT: the sub-FFT exchanges synchronise one warp (P = 512) or
+// their own T' threads, so double buffering saves little, while the 26 KB it costs at
+// P = 512 decides whether two blocks fit on an SM with 16 templates staged (measured on
+// B200: 8.5 instead of 9.4 us per template for the 1536-point pass).
+constexpr bool kXcorr3DB = false;
+
 template <int P, class ImgC, int FPB>
 struct Xcorr3Smem {
     static constexpr int kImgBytes = 3 * P * (int)sizeof(ImgC);
-    static constexpr int kXchBytes = Fft3Group<P, FPB, true>::BYTES;
+    static constexpr int kXchBytes = Fft3Group<P, FPB, kXcorr3DB>::BYTES;
     static __host__ __device__ constexpr int t1_col_elems(int L) { return (L + 1) & ~1; }  // 16-byte multiple
     static __host__ __device__ constexpr int img_off() { return 0; }
     static __host__ __device__ constexpr int xch_off() { return (kImgBytes + 127) & ~127; }
@@ -286,7 +292,7 @@ xcorr3_cols_kernel(XcorrColArgs a) {
 
     const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
     const int rounds = (a.n_batch + FPB - 1) / FPB;
-    Fft3Group<P, FPB, true> grp(xch, f, k2);
+    Fft3Group<P, FPB, kXcorr3DB> grp(xch, f, k2);
 #pragma unroll 1
     for (int it = 0; it < rounds; it++) {
         const int g = it * FPB + f;
