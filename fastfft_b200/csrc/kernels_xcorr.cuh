@@ -59,6 +59,8 @@ struct XcorrColArgs {
     const float2* tw3;         // N = 3P: radix-3 pass twiddles (set by the launcher)
     int* err;
     int L_g[kMaxBatch];        // per-template valid rows of uneven batches (0: use L)
+    int tpb;                   // templates per block: block (c, y) serves templates
+                               // [y tpb, min((y + 1) tpb, n_batch)) of column c (grid.y blocks)
 };
 
 // Shared-memory plan of the kernel (bytes), shared by the host launcher.
@@ -94,7 +96,9 @@ xcorr_cols_kernel(XcorrColArgs a) {
     const ImgC* img_s = reinterpret_cast<const ImgC*>(sm_raw + SM::img_off());
     float2* xch = reinterpret_cast<float2*>(sm_raw + SM::xch_off());
     float2* t1_s = reinterpret_cast<float2*>(sm_raw + SM::t1_off());
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm_raw + SM::bar_off(a.L, a.n_batch));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm_raw + SM::bar_off(a.L, a.tpb));
+    const int g0 = blockIdx.y * a.tpb;                              // first template of the block
+    const int nb = min(a.tpb, a.n_batch - g0);                      // templates of the block
 
     const int col = blockIdx.x;
     const int f = threadIdx.x / T;
@@ -103,29 +107,30 @@ xcorr_cols_kernel(XcorrColArgs a) {
 
     __shared__ int ok_flag;
     uint32_t bytes = (uint32_t)SM::kImgBytes;
-    for (int g = 0; g < a.n_batch; g++) bytes += (uint32_t)SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8;
+    for (int g = g0; g < g0 + nb; g++) bytes += (uint32_t)SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8;
     const bool staged = stage_block(bar, &ok_flag, bytes, a.err, [&]() {
         bulk_g2s(sm_raw + SM::img_off(), static_cast<const ImgC*>(a.img) + (long long)col * a.img_stride,
                  SM::kImgBytes, bar);
-        for (int g = 0; g < a.n_batch; g++)
-            bulk_g2s(t1_s + g * lcol, a.t1 + g * a.t1_batch + (long long)col * a.t1_pitch,
-                     SM::t1_col_elems(a.L_g[g] > 0 ? a.L_g[g] : a.L) * 8, bar);
+        for (int g = 0; g < nb; g++)
+            bulk_g2s(t1_s + g * lcol, a.t1 + (g0 + g) * a.t1_batch + (long long)col * a.t1_pitch,
+                     SM::t1_col_elems(a.L_g[g0 + g] > 0 ? a.L_g[g0 + g] : a.L) * 8, bar);
     });
     if (!staged) return;
 
     const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
-    const int rounds = (a.n_batch + FPB - 1) / FPB;
+    const int rounds = (nb + FPB - 1) / FPB;
     FftGroup<N, FPB, true> grp(xch, f);
 #pragma unroll 1
     for (int it = 0; it < rounds; it++) {
-        const int g = it * FPB + f;
-        const bool live = g < a.n_batch;
+        const int gl = it * FPB + f;                 // template within the block
+        const bool live = gl < nb;
+        const int g = g0 + (live ? gl : 0);          // template within the launch
         const int Lg = (live && a.L_g[g] > 0) ? a.L_g[g] : a.L;
         // keep the next template's loads from being scheduled into this template's
         // transforms (that would hold twice the values live and spill)
         asm volatile("" ::: "memory");
         float2 v[16];
-        const float2* src = t1_s + (live ? g : 0) * lcol;
+        const float2* src = t1_s + (live ? gl : 0) * lcol;
 #pragma unroll
         for (int q = 0; q < 16; q++) {
             const int n = j + T * q;

@@ -15,14 +15,15 @@ static cudaError_t xcorr_v2_impl(const XcorrColArgs& a, cudaStream_t st) {
         constexpr int FPB = col_fpb<N>();
         using SM = XcorrSmem<N, ImgC, FPB>;
         if (a.n_batch < 1 || a.n_batch > kMaxBatch || a.n_cols < 1) return cudaErrorInvalidValue;
-        const int smem = SM::total(a.L, a.n_batch);
+        if (a.tpb < 1 || a.tpb > a.n_batch) return cudaErrorInvalidValue;
+        const int smem = SM::total(a.L, a.tpb);
         if (smem > kMaxDynSmem) return cudaErrorInvalidValue;
         static std::atomic<int> set_mul[64], set_nomul[64];
         const bool mul = a.intra_kind != 0;
         auto fn = mul ? xcorr_cols_kernel<N, ImgC, FPB, true> : xcorr_cols_kernel<N, ImgC, FPB, false>;
         cudaError_t e = ensure_smem_at_least((const void*)fn, (size_t)smem, mul ? set_mul : set_nomul);
         if (e != cudaSuccess) return e;
-        fn<<<a.n_cols, FftShape<N>::T * FPB, smem, st>>>(a);
+        fn<<<dim3(a.n_cols, (a.n_batch + a.tpb - 1) / a.tpb), FftShape<N>::T * FPB, smem, st>>>(a);
         return cudaGetLastError();
     }
 }

@@ -165,3 +165,23 @@ def test_mixed_radix_templates_per_launch(torch_cuda, per_launch):
     for i in (0, 3, 6):
         ref = oracle_window(ts[i], fin, spec, fout, iout)
         assert O.rel_l2(O.real_from_padded(host(outs[i]), iout), ref) <= RTOL_L2_FP32
+
+
+def test_fused_pass_just_under_48k_shared_memory(torch_cuda):
+    """256^2 templates at 768^2, 8 per launch: the fused pass's dynamic shared memory is
+    49,040 B, under 48 KB by itself but over it with the kernel's static shared memory, so
+    the launcher has to raise the attribute."""
+    torch = torch_cuda
+    fin, fout, iout = (256, 256, 1), (1024, 1024, 1), (512, 512, 1)
+    ft = plan(fin, fout, iout)
+    ft.SetTemplatesPerLaunch(8)
+    assert ft.CorrelationSize() == (768, 768)
+    spec = image_spectrum(fout, 42)
+    d_spec = dev(torch, spec.view(np.float32))
+    rng = np.random.default_rng(43)
+    ts = [rng.standard_normal((256, 256)).astype(np.float32) for _ in range(8)]
+    outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    ft.FwdImageInvFFTMany([dev(torch, O.real_to_padded(t, fin)) for t in ts], d_spec, outs)
+    for i in (0, 7):
+        ref = oracle_window(ts[i], fin, spec, fout, iout)
+        assert O.rel_l2(O.real_from_padded(host(outs[i]), iout), ref) <= RTOL_L2_FP32
