@@ -68,6 +68,9 @@ SIGNATURES = {
     "fastfft_set_templates_per_launch": (_st, [Handle, ctypes.c_int]),
     "fastfft_fwd_image_inv_many_peaks": (_st, [Handle, ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int),
                                                ctypes.POINTER(_vp), ctypes.POINTER(_vp), _vp, _op, _op, _op]),
+    "fastfft_fwd_image_inv_many_mip": (_st, [Handle, ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(_vp), ctypes.POINTER(_vp), _vp, ctypes.c_int, _op, _op,
+                                             _op]),
     "fastfft_decode_peak": (None, [ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_float),
                                    ctypes.POINTER(ctypes.c_uint)]),
     "fastfft_templates_per_launch": (_st, [Handle, ctypes.POINTER(ctypes.c_int)]),

@@ -310,7 +310,7 @@ fastfft_status stage_r2c(fastfft_plan_s* h, int n, int in_dtype, const void* in,
 
 fastfft_status stage_c2r(fastfft_plan_s* h, int n, const float2* in, long long in_pitch, int n_rows, void* out,
                          long long out_pitch, int W, int X0, float scale, unsigned long long* peaks = nullptr,
-                         int peak_slot = 0) {
+                         int peak_slot = 0, unsigned long long* mip = nullptr, int mip_base = 0) {
     const float2* tw = nullptr;
     cudaError_t e = twiddles_for(n, &tw);
     if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
@@ -327,8 +327,10 @@ fastfft_status stage_c2r(fastfft_plan_s* h, int n, const float2* in, long long i
     a.scale = scale;
     a.tw = tw;
     a.peaks = peaks;
-    a.peaks_only = (peaks != nullptr && out == nullptr);
+    a.peaks_only = ((peaks != nullptr || mip != nullptr) && out == nullptr);
     a.peak_slot[0] = peak_slot;
+    a.mip = mip;
+    a.mip_base = mip_base;
     e = launch_c2r_rows(n, h->output_dtype, a, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "c2r row pass");
     h->launches++;
@@ -444,7 +446,8 @@ fastfft_status seq_inv(fastfft_plan_s* h, const void* in, int in_dtype, void* ou
 // 2D size-N fused correlation of one template of size (lx, ly) <= the plan's input size.
 fastfft_status seq_xcorr_sized(fastfft_plan_s* h, const void* in, int lx, int ly, const void* img, void* out,
                                float pre_scale, const fastfft_op* intra_op, float post_scale,
-                               unsigned long long* peaks = nullptr, int peak_slot = 0) {
+                               unsigned long long* peaks = nullptr, int peak_slot = 0,
+                               unsigned long long* mip = nullptr, int mip_base = 0) {
     const Dims &fo = h->fwd_out, &io = h->inv_out;
     const int nx = (int)fo.x, ny = (int)fo.y;
     const int kw = nx / 2 + 1;
@@ -458,7 +461,7 @@ fastfft_status seq_xcorr_sized(fastfft_plan_s* h, const void* in, int lx, int ly
     c.W0 = (int)h->org_y;
     FFB_TRY(stage_cols(h, ny, ST_XCORR, h->image_dtype, c));
     return stage_c2r(h, nx, region_b(h), h->pitch_b, (int)io.y, out, 2LL * io.w, (int)io.x, (int)h->org_x,
-                     post_scale, peaks, peak_slot);
+                     post_scale, peaks, peak_slot, mip, mip_base);
 }
 
 // Size-N fused correlation of one template (forward increase or no change).
@@ -734,7 +737,8 @@ static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spec
 static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const* inputs, const int* dims,
                                       void* const* outs, const fastfft_op* pre_op, const fastfft_op* intra_op,
                                       const fastfft_op* post_op, unsigned long long* peaks = nullptr,
-                                      const int* slots = nullptr) {
+                                      const int* slots = nullptr, unsigned long long* mip = nullptr,
+                                      int mip_base = 0) {
     const int mx = (int)h->red_mx, my = (int)h->red_my;
     char* c0 = region_c(h);
     const float2* spec = reinterpret_cast<const float2*>(c0 + h->off_c_spec);
@@ -788,10 +792,12 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const
     r.n_batch = n;
     r.in = t2; r.in_pitch = h->pitch_b; r.in_batch_stride = h->red_t2_stride; r.n_rows = (int)h->inv_out.y;
     for (int g = 0; g < n; g++) r.out[g] = outs[g];
-    if (peaks) {
+    if (peaks || mip) {
         r.peaks = peaks;
         r.peaks_only = outs[0] == nullptr;
         for (int g = 0; g < n; g++) r.peak_slot[g] = slots[g];
+        r.mip = mip;
+        r.mip_base = mip_base;
     }
     r.out_pitch = 2LL * h->inv_out.w; r.W = (int)h->inv_out.x; r.scale = scale_of(post_op); r.tw = tw;
     if ((e = launch_c2r_rows(mx, h->output_dtype, r, h->stream)) != cudaSuccess)
@@ -816,7 +822,10 @@ fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const 
 static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inputs, const int* dims,
                                  const void* const* image_spectra, void* const* outputs, const fastfft_op* pre_op,
                                  const fastfft_op* intra_op, const fastfft_op* post_op,
-                                 unsigned long long* peaks = nullptr) {
+                                 unsigned long long* peaks = nullptr, unsigned long long* mip = nullptr,
+                                 int mip_base = 0) {
+    // with a peak array or a projection the windows are written only where outputs[i] is set
+    const bool reduce = peaks != nullptr || mip != nullptr;
     if (n < 0 || (n > 0 && (!inputs || !image_spectra)))
         return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image array");
     for (int i = 0; i < n; i++)
@@ -837,13 +846,13 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
     }
     if (!h->red_ok || h->force_full_size) {
         for (int i = 0; i < n; i++) {
-            void* out = peaks ? (outputs ? outputs[i] : nullptr)
-                              : ((outputs && outputs[i]) ? outputs[i] : const_cast<void*>(inputs[i]));
-            if (dims || peaks) {
+            void* out = reduce ? (outputs ? outputs[i] : nullptr)
+                               : ((outputs && outputs[i]) ? outputs[i] : const_cast<void*>(inputs[i]));
+            if (dims || reduce) {
                 prof_begin_call(h);
                 st = seq_xcorr_sized(h, inputs[i], dims ? dims[2 * i] : (int)h->fwd_in.x,
                                      dims ? dims[2 * i + 1] : (int)h->fwd_in.y, image_spectra[i], out,
-                                     scale_of(pre_op), intra_op, scale_of(post_op), peaks, i);
+                                     scale_of(pre_op), intra_op, scale_of(post_op), peaks, i, mip, mip_base);
                 prof_end_call(h);
             } else {
                 st = xcorr_one(h, inputs[i], image_spectra[i], out, pre_op, intra_op, post_op);
@@ -868,8 +877,8 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
         for (int k = i; k < n; k++) {
             if (done[k] || image_spectra[k] != img) continue;
             grp_in[m] = inputs[k];
-            grp_out[m] = peaks ? (outputs ? outputs[k] : nullptr)
-                               : ((outputs && outputs[k]) ? outputs[k] : const_cast<void*>(inputs[k]));
+            grp_out[m] = reduce ? (outputs ? outputs[k] : nullptr)
+                                : ((outputs && outputs[k]) ? outputs[k] : const_cast<void*>(inputs[k]));
             grp_slot[m] = k;
             if (dims) {
                 grp_dims[2 * m] = dims[2 * k];
@@ -878,14 +887,14 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
             done[k] = 1;
             if (++m == h->red_batch) {
                 st = red_xcorr_batch(h, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op, post_op,
-                                     peaks, grp_slot);
+                                     peaks, grp_slot, mip, mip_base);
                 if (st != FASTFFT_OK) return st;
                 m = 0;
             }
         }
         if (m > 0) {
             st = red_xcorr_batch(h, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op, post_op,
-                                 peaks, grp_slot);
+                                 peaks, grp_slot, mip, mip_base);
             if (st != FASTFFT_OK) return st;
         }
     }
@@ -921,6 +930,23 @@ fastfft_status fastfft_fwd_image_inv_many_peaks(fastfft_handle h, int n, const v
         for (int i = 0; i < n; i++)
             if (!outputs[i]) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null output pointer in the batch");
     return xcorr_many(h, n, inputs, template_dims, image_spectra, outputs, pre_op, intra_op, post_op, peaks);
+}
+
+fastfft_status fastfft_fwd_image_inv_many_mip(fastfft_handle h, int n, const void* const* inputs,
+                                              const int* template_dims, const void* const* image_spectra,
+                                              void* const* outputs, unsigned long long* mip, int index_base,
+                                              const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                              const fastfft_op* post_op) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (n > 0 && !mip) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null projection array");
+    if (h->rank != 2) return fail(h, FASTFFT_ERR_UNSUPPORTED, "the fused maximum projection is 2D only");
+    if (index_base < 0 || (long long)index_base + n > 0x7FFFFFFFLL)
+        return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "template indices must be in [0, 2^31)");
+    if (outputs)
+        for (int i = 0; i < n; i++)
+            if (!outputs[i]) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null output pointer in the batch");
+    return xcorr_many(h, n, inputs, template_dims, image_spectra, outputs, pre_op, intra_op, post_op, nullptr, mip,
+                      index_base);
 }
 
 fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n) {

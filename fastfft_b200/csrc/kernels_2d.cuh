@@ -284,8 +284,13 @@ struct RowInvArgs {
     // window and its first flat index (row * W + x) are folded into peaks[g] as a
     // peak_key(); with peaks_only the window itself is not written.
     unsigned long long* peaks;
-    int peaks_only;
+    int peaks_only;            // the windows are not written (peak search or projection only)
     int peak_slot[kMaxBatch];  // batch entry g folds into peaks[peak_slot[g]]
+    // Fused maximum projection across templates: if mip is set, every retained pixel
+    // (row r, x) of batch entry g folds peak_key(value, mip_base + peak_slot[g]) into
+    // mip[r * W + x] (the best value over the templates and its first template).
+    unsigned long long* mip;
+    int mip_base;
 };
 
 // Total order on (value, index) for a 64-bit atomicMax: larger value wins, and among
@@ -365,6 +370,18 @@ c2r_rows_kernel(RowInvArgs a) {
             if (n >= 0 && n < a.W) {
                 if (has_a) st_real<OutT>(oa + n, v[q].x * a.scale);
                 if (has_b) st_real<OutT>(ob + n, v[q].y * a.scale);
+            }
+        }
+    }
+    if (a.mip) {
+        const unsigned int tmpl = (unsigned)(a.mip_base + a.peak_slot[blockIdx.y]);
+        unsigned long long* ma = a.mip + (long long)ra * a.W;
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int n = j + T * q - a.X0;
+            if (n >= 0 && n < a.W) {
+                if (has_a) atomicMax(ma + n, peak_key(v[q].x * a.scale, tmpl));
+                if (has_b) atomicMax(ma + a.W + n, peak_key(v[q].y * a.scale, tmpl));
             }
         }
     }

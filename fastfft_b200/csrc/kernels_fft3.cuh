@@ -166,6 +166,8 @@ c2r3_rows_kernel(RowInvArgs a) {
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
     const bool write = !a.peaks_only;
     unsigned long long best = 0;
+    const unsigned int tmpl = (unsigned)(a.mip_base + a.peak_slot[blockIdx.y]);
+    unsigned long long* ma = a.mip ? a.mip + (long long)ra * a.W : nullptr;
     dit_output<P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
         const int n = n0 - a.X0;
         if (n >= 0 && n < a.W) {
@@ -173,6 +175,10 @@ c2r3_rows_kernel(RowInvArgs a) {
             if (write) {
                 if (has_a) st_real<OutT>(oa + n, va);
                 if (has_b) st_real<OutT>(ob + n, vb);
+            }
+            if (ma) {
+                if (has_a) atomicMax(ma + n, peak_key(va, tmpl));
+                if (has_b) atomicMax(ma + a.W + n, peak_key(vb, tmpl));
             }
             if (a.peaks) {
                 if (has_a) {

@@ -210,6 +210,33 @@ class FourierTransformer:
         self._check(self._lib.fastfft_fwd_image_inv_many_peaks(self._h, n, ins, dims, ims, outs, _ptr(peaks),
                                                                _opref(pre_op), _opref(intra_op), _opref(post_op)))
 
+    def FwdImageInvFFTManyMip(self, inputs, images, mip, sizes=None, outputs=None, index_base=0, pre_op=None,
+                              intra_op=None, post_op=None):
+        """Batched correlation with a fused maximum projection across templates: every
+        retained pixel of mip (int64 CUDA tensor of out_x * out_y keys, row-major; zero it
+        before the first call) keeps the best score over the templates and its template
+        number index_base + i (decode with decode_peaks).  The array accumulates across
+        calls.  outputs None: the windows are not written."""
+        n = len(inputs)
+        if not isinstance(images, (list, tuple)):
+            images = [images] * n
+        if len(images) != n or (outputs is not None and len(outputs) != n) or (sizes is not None and len(sizes) != n):
+            raise ValueError("inputs, images, sizes and outputs must have the same length")
+        out_x, out_y = self.ReturnInvOutputDimensions()[:2]
+        if mip.numel() < out_x * out_y or mip.element_size() != 8:
+            raise ValueError("mip must hold one 64-bit value per window pixel (out_x * out_y)")
+        if intra_op is None:
+            intra_op = KernelFunction.conj_mul()
+        arr = ctypes.c_void_p * n
+        dims = (ctypes.c_int * (2 * n))(*[int(v) for xy in sizes for v in xy]) if sizes is not None else None
+        ins = arr(*[_ptr(x) for x in inputs])
+        ims = arr(*[_ptr(x) for x in images])
+        outs = arr(*[_ptr(x) for x in outputs]) if outputs is not None else None
+        self._bind_stream()
+        self._check(self._lib.fastfft_fwd_image_inv_many_mip(self._h, n, ins, dims, ims, outs, _ptr(mip),
+                                                             int(index_base), _opref(pre_op), _opref(intra_op),
+                                                             _opref(post_op)))
+
     def SetTemplatesPerLaunch(self, n):
         self._check(self._lib.fastfft_set_templates_per_launch(self._h, int(n)))
 

@@ -142,7 +142,22 @@ FASTFFT_API fastfft_status fastfft_fwd_image_inv_many_peaks(fastfft_handle h, in
                                                             const void* const* image_spectra, void* const* outputs,
                                                             unsigned long long* peaks, const fastfft_op* pre_op,
                                                             const fastfft_op* intra_op, const fastfft_op* post_op);
-/* Host-side decode of one peaks[] entry. */
+/* Batched correlation with a fused maximum projection across templates (the per-pixel
+ * best score and best template of a template search): for every retained pixel (y, x) of
+ * every template i of the call, mip[y * out_x + x] (device memory, out_x * out_y values)
+ * is raised to the key of (score, index_base + i), packed as for the peak search with the
+ * template number in place of the pixel index; the larger score wins and, on equal
+ * scores, the smaller template number.  The array is not cleared: zero it once, then
+ * stream any number of calls into it, numbering their templates with index_base.
+ * outputs NULL: the windows are not written.  template_dims may be NULL (plan size).  No
+ * reference counterpart. */
+FASTFFT_API fastfft_status fastfft_fwd_image_inv_many_mip(fastfft_handle h, int n, const void* const* inputs,
+                                                          const int* template_dims,
+                                                          const void* const* image_spectra, void* const* outputs,
+                                                          unsigned long long* mip, int index_base,
+                                                          const fastfft_op* pre_op, const fastfft_op* intra_op,
+                                                          const fastfft_op* post_op);
+/* Host-side decode of one peaks[] or mip[] entry. */
 FASTFFT_API void fastfft_decode_peak(unsigned long long key, float* value, unsigned int* index);
 
 /* Templates per launch of the batched reduced-size path (1..16, default 8; lowered if the
@@ -150,8 +165,8 @@ FASTFFT_API void fastfft_decode_peak(unsigned long long key, float* value, unsig
 FASTFFT_API fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n);
 FASTFFT_API fastfft_status fastfft_templates_per_launch(fastfft_handle h, int* n);
 
-/* The batched call correlates at the smallest power-of-two size M >= L + W - 1 per axis
- * when that is below the plan's N (template in [0, L), window in [0, W)): every
+/* The batched call correlates at the smallest supported size M >= L + W - 1 per axis (a
+ * power of two, or 3 * 2^k with 128 <= 2^k <= 2048) when that is below the plan's N (template in [0, L), window in [0, W)): every
  * retained lag then reads image pixels in [0, L + W - 1) only, so the size-M
  * circular correlation against the spectrum of the image cropped to [0, M) gives the
  * same values as the size-N one.  Each distinct image in a call is prepared once.
