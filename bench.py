@@ -465,6 +465,41 @@ def run_ours(args, world, rank, local):
     pk_ms = max_over_ranks(world, f0.elapsed_time(f1), torch, dev)
     pk_value = world * e2e_steps * B / (pk_ms * 1e-3)
 
+    # the same through the fused maximum projection (a template search's per-pixel best
+    # score and best template): each step searches its image with the step's templates and
+    # reads the W x W projection back (8 bytes per pixel per step, not per template)
+    mip = torch.zeros(W * W, dtype=torch.int64, device=dev)
+    h_mip = torch.empty(W * W, dtype=torch.int64, pin_memory=True)
+
+    def e2e_mip(n_steps):
+        with torch.cuda.stream(copy):
+            d_tpl[0].copy_(h_in, non_blocking=True)
+            uploaded[0].record(copy)
+        for s in range(n_steps):
+            k = s % 2
+            if s + 1 < n_steps:
+                with torch.cuda.stream(copy):
+                    if s >= 1:
+                        copy.wait_event(consumed[1 - k])
+                    d_tpl[1 - k].copy_(h_in, non_blocking=True)
+                    uploaded[1 - k].record(copy)
+            main.wait_event(uploaded[k])
+            mip.zero_()
+            ft.FwdImageInvFFTManyMip(ins2[k], images[s % N_IMAGES], mip, index_base=0)
+            consumed[k].record(main)
+            h_mip.copy_(mip, non_blocking=True)
+        main.wait_stream(copy)
+
+    e2e_mip(2)
+    torch.cuda.synchronize()
+    barrier(world, torch)
+    f0.record()
+    e2e_mip(e2e_steps)
+    f1.record()
+    torch.cuda.synchronize()
+    mip_ms = max_over_ranks(world, f0.elapsed_time(f1), torch, dev)
+    mip_value = world * e2e_steps * B / (mip_ms * 1e-3)
+
     # ---- cuFFT pad-then-transform comparator (torch.fft) ----
     cufft = None
     if rank == 0 and not args.skip_cufft:
@@ -547,6 +582,10 @@ def run_ours(args, world, rank, local):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": B * n_in * 4,
                     "d2h_bytes_per_step": B * n_out * 4, "steps": e2e_steps,
                     "how": "FwdImageInvFFTMany; pinned-host templates in, 1024^2 windows out on an overlapped copy stream"},
+            "e2e_mip": {"value": mip_value, "unit": UNIT, "h2d_bytes_per_step": B * n_in * 4,
+                        "d2h_bytes_per_step": W * W * 8,
+                        "how": "FwdImageInvFFTManyMip: per-pixel best score and best template over the step's "
+                               "templates, read back once per step; windows not written"},
             "e2e_peaks": {"value": pk_value, "unit": UNIT, "h2d_bytes_per_step": B * n_in * 4,
                           "d2h_bytes_per_step": B * 8,
                           "how": "FwdImageInvFFTManyPeaks: window max and argmax per template, windows not written"},

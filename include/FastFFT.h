@@ -186,6 +186,26 @@ class FourierTransformer {
               "FwdImageInvFFTMany");
     }
 
+    // Extension: many templates of uneven sizes (sizes[2i], sizes[2i+1] = x, y; may be null
+    // for the plan size) with the fused per-pixel maximum projection into mip (device memory,
+    // one 64-bit key per window pixel; see fastfft_fwd_image_inv_many_mip).  outputs may be
+    // null (windows not written).
+    template <class PreOpType = std::nullptr_t, class IntraOpType = std::nullptr_t,
+              class PostOpType = std::nullptr_t>
+    void FwdImageInvFFTManyMip(int n, InputType* const* inputs, const int* sizes, OtherImageType* const* images,
+                               InputType* const* outputs, unsigned long long* mip, int index_base = 0,
+                               PreOpType pre_op = nullptr, IntraOpType intra_op = nullptr,
+                               PostOpType post_op = nullptr) {
+        std::vector<const void*> in(inputs, inputs + n), im(images, images + n);
+        std::vector<void*> out;
+        if (outputs) out.assign(outputs, outputs + n);
+        fastfft_op a, b, c;
+        check(fastfft_fwd_image_inv_many_mip(h_, n, in.data(), sizes, im.data(), outputs ? out.data() : nullptr, mip,
+                                             index_base, detail::op_ptr(pre_op, a), detail::op_ptr(intra_op, b),
+                                             detail::op_ptr(post_op, c)),
+              "FwdImageInvFFTManyMip");
+    }
+
     int ReturnInputMemorySize() { return static_cast<int>(ll(fastfft_input_memory_size)); }
     int ReturnFwdOutputMemorySize() { return static_cast<int>(ll(fastfft_fwd_output_memory_size)); }
     int ReturnInvOutputMemorySize() { return static_cast<int>(ll(fastfft_inv_output_memory_size)); }

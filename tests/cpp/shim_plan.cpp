@@ -5,7 +5,7 @@
 
 #include "FastFFT.h"
 
-int main() {
+int main(int argc, char**) {
     FastFFT::FourierTransformer<float, float, float2, 2> ft;
     ft.SetForwardFFTPlan(384, 384, 1, 4096, 4096, 1, true);
     ft.SetInverseFFTPlan(4096, 4096, 1, 1024, 1024, 1, true);
@@ -13,6 +13,11 @@ int main() {
     std::printf("%d %d %d %d %d %d %d %d\n", ft.ReturnInputMemorySize(), ft.ReturnFwdOutputMemorySize(),
                 ft.ReturnInvOutputMemorySize(), (int)o.x, (int)o.y, (int)o.z, (int)o.w,
                 (int)ft.ReturnInvOutputDimensions().w);
+    if (argc > 99) {  // compiled but never run here: type-checks the batched extensions
+        FastFFT::KernelFunction::my_functor<float, 4, FastFFT::KernelFunction::CONJ_MUL> conj_mul;
+        ft.FwdImageInvFFTMany(0, nullptr, nullptr, nullptr, nullptr, conj_mul, nullptr);
+        ft.FwdImageInvFFTManyMip(0, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, conj_mul, nullptr);
+    }
     FastFFT::FourierTransformer<float, __half, __half2, 3> ft3;
     ft3.SetForwardFFTPlan(64, 64, 64, 256, 256, 256);
     try {
