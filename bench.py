@@ -292,6 +292,50 @@ def run_uneven(dev, image_f32, storage="float32", reps=5):
             "template_edge_counts": {str(k): int((edges == k).sum()) for k in UNEVEN_SIZES}}
 
 
+def run_low_precision(dev, images_f32, templates_f32, storage, steps, warmup=3):
+    """The headline workload with the templates and the image spectra stored in FP16 or
+    BF16 (image spectra scaled by 1/4096 before rounding, the overflow guard), FP32
+    arithmetic and FP32 windows; same steps as the main leg (B templates per step, image
+    spectra rotating).  Returns the result and, for the accuracy check, template 0's window
+    with the dequantized template and image 0."""
+    import torch
+
+    import fastfft_b200 as F
+    from fastfft_b200.autotune import tune
+
+    tdt = torch.float16 if storage == "float16" else torch.bfloat16
+    ft = F.FourierTransformer(input_dtype=storage, image_dtype="complex32" if storage == "float16" else "complex_bf16")
+    ft.SetForwardFFTPlan(L, L, 1, N, N, 1)
+    ft.SetInverseFFTPlan(N, N, 1, W, W, 1)
+    ft.SetOutputDtype("float32")
+    B = templates_f32.shape[0]
+    images = [(im * (1.0 / N)).to(tdt) for im in images_f32]
+    templates = templates_f32.to(tdt)
+    outputs = torch.empty(B, ft.ReturnInvOutputMemorySize(), dtype=torch.float32, device=dev)
+    ins = [templates[i] for i in range(B)]
+    outs = [outputs[i] for i in range(B)]
+    per_launch = tune(ft, ins, images[0], outs)
+    for i in range(warmup):
+        ft.FwdImageInvFFTMany(ins, images[i % len(images)], outs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(steps):
+        ft.FwdImageInvFFTMany(ins, images[i % len(images)], outs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ft.FwdImageInvFFTMany(ins[:1], images[0], outs[:1])
+    torch.cuda.synchronize()
+    result = {"storage": storage, "value": steps * B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
+              "correlation_size": list(ft.CorrelationSize()), "templates_per_launch": per_launch,
+              "how": "templates and image spectra stored in " + storage + " (image spectra scaled by 1/4096), "
+                     "FP32 arithmetic, FP32 windows"}
+    check = {"window": outputs[0].cpu().numpy(), "template": templates[0].float().cpu().numpy(),
+             "image": images[0].float().cpu().numpy()}
+    return result, check
+
+
 # ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
@@ -468,8 +512,12 @@ def run_ours(args, world, rank, local):
     # the same through the fused maximum projection (a template search's per-pixel best
     # score and best template): each step searches its image with the step's templates and
     # reads the W x W projection back (8 bytes per pixel per step, not per template)
-    mip = torch.zeros(W * W, dtype=torch.int64, device=dev)
-    h_mip = torch.empty(W * W, dtype=torch.int64, pin_memory=True)
+    # two projection buffers: step s searches into mips[s % 2] while the copy stream reads
+    # the previous step's projection back
+    mips = [torch.zeros(W * W, dtype=torch.int64, device=dev) for _ in range(2)]
+    h_mip = [torch.empty(W * W, dtype=torch.int64, pin_memory=True) for _ in range(2)]
+    searched = [torch.cuda.Event() for _ in range(2)]
+    read_back = [torch.cuda.Event() for _ in range(2)]
 
     def e2e_mip(n_steps):
         with torch.cuda.stream(copy):
@@ -484,10 +532,16 @@ def run_ours(args, world, rank, local):
                     d_tpl[1 - k].copy_(h_in, non_blocking=True)
                     uploaded[1 - k].record(copy)
             main.wait_event(uploaded[k])
-            mip.zero_()
-            ft.FwdImageInvFFTManyMip(ins2[k], images[s % N_IMAGES], mip, index_base=0)
+            if s >= 2:
+                main.wait_event(read_back[k])
+            mips[k].zero_()
+            ft.FwdImageInvFFTManyMip(ins2[k], images[s % N_IMAGES], mips[k], index_base=0)
             consumed[k].record(main)
-            h_mip.copy_(mip, non_blocking=True)
+            searched[k].record(main)
+            with torch.cuda.stream(copy):
+                copy.wait_event(searched[k])
+                h_mip[k].copy_(mips[k], non_blocking=True)
+                read_back[k].record(copy)
         main.wait_stream(copy)
 
     e2e_mip(2)
@@ -531,6 +585,16 @@ def run_ours(args, world, rank, local):
     if rank == 0 and not args.skip_uneven:
         uneven = [run_uneven(dev, images[0], "float32"), run_uneven(dev, images[0], "bfloat16")]
 
+    # ---- the headline workload with FP16 / BF16 storage (rank 0) ----
+    low = None
+    low_checks = {}
+    if rank == 0 and not args.skip_uneven:
+        low = []
+        for storage in ("float16", "bfloat16"):
+            r, chk = run_low_precision(dev, images, templates, storage, args.steps)
+            low.append(r)
+            low_checks[storage] = chk
+
     # ---- CPU baseline (rank 0, one GPU) and accuracy check of one window ----
     cpu = None
     accuracy = None
@@ -560,6 +624,16 @@ def run_ours(args, world, rank, local):
         ri, rtop, margin = O.peak(ref)
         accuracy = {"rel_l2_vs_fp64": O.rel_l2(got, ref), "rel_max_vs_fp64": O.rel_max(got, ref),
                     "peak_index_exact": bool(gi == ri), "peak_margin_rel": margin / abs(rtop)}
+        # low-precision storage: against the FP64 oracle of the dequantized template and image
+        # (the rounding of the stored inputs is the caller's choice; the path adds FP32 error
+        # only), and the peak index against the FP32 path's
+        for r in low or []:
+            chk = low_checks[r["storage"]]
+            spec_q = chk["image"].view(np.complex64).reshape(1, N // 2 + 1, N)
+            ref_q = O.real_from_padded(O.fwd_image_inv(chk["template"], spec_q, plan, out_dtype=np.float64), (W, W, 1))
+            got_q = O.real_from_padded(chk["window"], (W, W, 1))
+            r["accuracy"] = {"rel_l2_vs_fp64_of_stored_inputs": O.rel_l2(got_q, ref_q),
+                             "peak_index_equals_fp32_path": bool(O.peak(got_q)[0] == gi)}
 
     if rank == 0:
         line = {
@@ -593,7 +667,7 @@ def run_ours(args, world, rank, local):
             "clocks": clk,
             "cufft_pad_then_transform": cufft,
             "accuracy": accuracy,
-            "uneven_batch": uneven,
+            "uneven_batch": uneven, "low_precision_storage": low,
         }
         print(json.dumps(line), flush=True)
 
@@ -601,7 +675,7 @@ def run_ours(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--templates-per-step", type=int, default=TEMPLATES_PER_STEP)
