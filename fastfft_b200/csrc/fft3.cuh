@@ -51,6 +51,10 @@ struct Fft3Shape {
     static constexpr int TP = P / 16;                  // threads per sub-FFT
     static constexpr int T = 3 * TP;                   // threads per FFT
     static constexpr int SUB = FftShape<P>::SMEM_PAD;  // float2 per sub-FFT region
+    // Region stride of the row C2R, which writes its input spectrum decimated by 3 (Z[k] in
+    // region k % 3 at phys(k / 3)): 5 past a multiple of 16 keeps both that scatter and the
+    // sub-FFTs' unit-stride loads within one or two shared-memory wavefronts per access.
+    static constexpr int SUB_C2R = (FftShape<P>::SMEM + 15) / 16 * 16 + 5;
     static constexpr int SMEM = 3 * SUB;               // float2 per exchange buffer
     static constexpr int ROUNDS = (P + T - 1) / T;     // radix-3 items per thread (6)
 };
@@ -72,12 +76,15 @@ __device__ __forceinline__ int loc3(int k) {
 // Every buffer that the radix-3 step reads across regions is rewritten only after a
 // sync_fft() that all its readers passed (the kernels call sync_fft() where a sub-FFT
 // exchange follows such reads).  Double buffering (DB) as in FftGroup.
-template <int P, int FPB, bool DB>
+template <int P, int FPB, bool DB, int SUBX = Fft3Shape<P>::SUB>
 struct Fft3Group {
     using S3 = Fft3Shape<P>;
     static constexpr int T = S3::T;
     static constexpr int TP = S3::TP;
-    static constexpr int STRIDE = (DB ? 2 : 1) * S3::SMEM;
+    static_assert(SUBX >= FftShape<P>::SMEM, "a region must hold one sub-FFT's exchange");
+    static constexpr int SUB = SUBX;                  // region stride (float2)
+    static constexpr int SMEM = 3 * SUBX;             // float2 per exchange buffer
+    static constexpr int STRIDE = (DB ? 2 : 1) * SMEM;
     static constexpr int BYTES = FPB * STRIDE * (int)sizeof(float2);
     static_assert(TP <= 32 || 4 * FPB <= 15, "named barriers: FFT ids 1..FPB, sub-FFT ids FPB+1..4 FPB");
     float2* base;
@@ -107,7 +114,7 @@ struct Fft3Group {
     __device__ __forceinline__ float2* next_buffer(bool sub_level) {
         float2* p = base;
         if constexpr (DB) {
-            p += (k & 1) * S3::SMEM;
+            p += (k & 1) * SMEM;
         } else {
             if (sub_level) sync(); else sync_fft();
         }
@@ -116,7 +123,7 @@ struct Fft3Group {
     }
 
     __device__ __forceinline__ float2* begin_full() { return next_buffer(false); }
-    __device__ __forceinline__ float2* begin() { return next_buffer(true) + r * S3::SUB; }
+    __device__ __forceinline__ float2* begin() { return next_buffer(true) + r * SUB; }
 };
 
 constexpr float kH3 = 0.866025403784438646764f;  // sqrt(3)/2
@@ -158,7 +165,7 @@ __device__ __forceinline__ void dit_output(float2 (&v)[16], G& g, int j, int t, 
     using S3 = Fft3Shape<P>;
     float2* buf = g.begin_full();
     {
-        float2* s = buf + g.r * S3::SUB;
+        float2* s = buf + g.r * G::SUB;
 #pragma unroll
         for (int q = 0; q < 16; q++) s[phys(j + S3::TP * q)] = v[q];
     }
@@ -169,8 +176,8 @@ __device__ __forceinline__ void dit_output(float2 (&v)[16], G& g, int j, int t, 
         if (n1 < P) {
             const int p = phys(n1);
             float2 a = buf[p];
-            float2 b = cmulc(buf[S3::SUB + p], ld_tw(tw3 + n1));
-            float2 c = cmulc(buf[2 * S3::SUB + p], ld_tw(tw3 + 2 * n1));
+            float2 b = cmulc(buf[G::SUB + p], ld_tw(tw3 + n1));
+            float2 c = cmulc(buf[2 * G::SUB + p], ld_tw(tw3 + 2 * n1));
             idft3(a, b, c);
             store(n1, a);
             store(n1 + P, b);
@@ -192,7 +199,7 @@ __device__ __forceinline__ float2* forward_dit(float2 (&v)[16], G& g, int j, int
     BlockFft<P, false>::run(v, g, j, tw, qnz);
     float2* buf = g.begin_full();
     {
-        float2* s = buf + g.r * S3::SUB;
+        float2* s = buf + g.r * G::SUB;
 #pragma unroll
         for (int q = 0; q < 16; q++) s[phys(j + S3::TP * q)] = v[q];
     }
@@ -203,11 +210,11 @@ __device__ __forceinline__ float2* forward_dit(float2 (&v)[16], G& g, int j, int
         if (k1 < P) {
             const int p = phys(k1);
             const float2 a = buf[p];
-            const float2 b = cmul(buf[S3::SUB + p], ld_tw(tw3 + k1));
-            const float2 c = cmul(buf[2 * S3::SUB + p], ld_tw(tw3 + 2 * k1));
+            const float2 b = cmul(buf[G::SUB + p], ld_tw(tw3 + k1));
+            const float2 c = cmul(buf[2 * G::SUB + p], ld_tw(tw3 + 2 * k1));
             buf[p] = dft3_component(a, b, c, 0);
-            buf[S3::SUB + p] = dft3_component(a, b, c, 1);
-            buf[2 * S3::SUB + p] = dft3_component(a, b, c, 2);
+            buf[G::SUB + p] = dft3_component(a, b, c, 1);
+            buf[2 * G::SUB + p] = dft3_component(a, b, c, 2);
         }
     }
     g.sync_fft();

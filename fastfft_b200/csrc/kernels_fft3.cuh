@@ -107,7 +107,10 @@ c2r3_rows_kernel(RowInvArgs a) {
     constexpr int TP = S3::TP;
     constexpr int H = N / 2;
     extern __shared__ float2 smem[];
-    using G = Fft3Group<P, FPB, false>;
+    using G = Fft3Group<P, FPB, false, S3::SUB_C2R>;
+    // Z[k] of FFT ff at sf[dec(k)]: decimated by 3, so that sub-FFT k2 finds its inputs
+    // Z[3 m + k2] contiguous in its own region
+    auto dec = [](int k) { return (k % 3) * G::SUB + phys(k / 3); };
     const int f = threadIdx.x / T;
     const int t = threadIdx.x - f * T;
     const int k2 = t / TP;
@@ -144,21 +147,22 @@ c2r3_rows_kernel(RowInvArgs a) {
             const float2 A = make_float2(ld[it].x, ld[it].y), B = make_float2(ld[it].z, ld[it].w);
             float2* sf = smem + ff * G::STRIDE;
             if (k == 0 || k == H) {
-                sf[loc3<P>(k)] = make_float2(A.x, B.x);
+                sf[dec(k)] = make_float2(A.x, B.x);
             } else {
-                sf[loc3<P>(k)] = make_float2(A.x - B.y, A.y + B.x);
-                sf[loc3<P>(N - k)] = make_float2(A.x + B.y, B.x - A.y);
+                sf[dec(k)] = make_float2(A.x - B.y, A.y + B.x);
+                sf[dec(N - k)] = make_float2(A.x + B.y, B.x - A.y);
             }
         }
     }
     __syncthreads();
     float2 v[16];
     {
-        const float2* z = g.base;
+        const float2* z = g.base + k2 * G::SUB;
 #pragma unroll
-        for (int q = 0; q < 16; q++) v[q] = z[loc3<P>(3 * (j + TP * q) + k2)];
+        for (int q = 0; q < 16; q++) v[q] = z[phys(j + TP * q)];
     }
-    g.sync_fft();  // the reads above cross regions; the sub-FFT exchanges rewrite them
+    // (each sub-FFT read only its own region, which its first exchange rewrites after its
+    // own barrier)
     BlockFft<P, true>::run(v, g, j, a.tw, 16);
     const int ra = 2 * (blockIdx.x * FPB + f);
     OutT* oa = static_cast<OutT*>(a.out[blockIdx.y]) + (long long)ra * a.out_pitch;

@@ -82,7 +82,7 @@ template <int P, class OutT>
 static cudaError_t c2r3_impl(const RowInvArgs& a0, cudaStream_t st) {
     constexpr int FPB = row_fpb3<P>();
     constexpr int THREADS = Fft3Shape<P>::T * FPB;
-    const size_t smem = (size_t)Fft3Group<P, FPB, false>::BYTES;
+    const size_t smem = (size_t)Fft3Group<P, FPB, false, Fft3Shape<P>::SUB_C2R>::BYTES;
     RowInvArgs a = a0;
     cudaError_t e = tables3(P, &a.tw, &a.tw3);
     if (e != cudaSuccess) return e;
