@@ -37,6 +37,7 @@ def oracle_window(t, fin, spec, fout, iout):
 # (template, transform, window, expected correlation size)
 CASES3 = [
     ((96, 96, 1), (1024, 1024, 1), (256, 256, 1), (384, 384)),        # 351 -> 3 * 128
+    ((200, 200, 1), (1024, 1024, 1), (150, 150, 1), (384, 384)),      # 349 -> 3 * 128, template longer than P
     ((200, 150, 1), (1024, 1024, 1), (500, 600, 1), (768, 768)),      # 699, 749 -> 3 * 256
     ((384, 384, 1), (2048, 2048, 1), (1024, 1024, 1), (1536, 1536)),  # 1407 -> 3 * 512
     ((1000, 16, 1), (4096, 64, 1), (2000, 16, 1), (3072, 32)),        # 2999 -> 3 * 1024 along x
