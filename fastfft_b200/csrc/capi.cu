@@ -154,6 +154,7 @@ long long corr_size_at_least(long long v) {
 }
 
 void size_buffers(fastfft_plan_s* h) {
+    h->prepared_image = nullptr;
     const long long nx_f = std::max(h->fwd_in.x, h->fwd_out.x);
     const long long kx_f = nx_f / 2 + 1;
     const long long kx_i = h->inv_in.x / 2 + 1;
@@ -614,7 +615,16 @@ fastfft_status fastfft_set_inverse_plan(fastfft_handle h, size_t ix, size_t iy, 
 
 fastfft_status fastfft_set_stream(fastfft_handle h, void* cuda_stream) {
     if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
-    h->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : cudaStreamPerThread;
+    cudaStream_t s = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : cudaStreamPerThread;
+    if (s != h->stream) h->prepared_image = nullptr;  // a preparation may still run on the old stream
+    h->stream = s;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_set_image_reuse(fastfft_handle h, int enable) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    h->image_reuse = enable != 0;
+    h->prepared_image = nullptr;
     return FASTFFT_OK;
 }
 
@@ -696,6 +706,12 @@ static fastfft_status xcorr_checks(fastfft_handle h, const fastfft_op* pre_op, c
     return FASTFFT_OK;
 }
 
+static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inputs, const int* dims,
+                                 const void* const* image_spectra, void* const* outputs, const fastfft_op* pre_op,
+                                 const fastfft_op* intra_op, const fastfft_op* post_op,
+                                 unsigned long long* peaks = nullptr, unsigned long long* mip = nullptr,
+                                 int mip_base = 0);
+
 static fastfft_status xcorr_one(fastfft_handle h, const void* input, const void* image_spectrum, void* out,
                                 const fastfft_op* pre_op, const fastfft_op* intra_op, const fastfft_op* post_op) {
     prof_begin_call(h);
@@ -708,6 +724,8 @@ static fastfft_status xcorr_one(fastfft_handle h, const void* input, const void*
 // [0, My) x [0, Mx), R2C at size M, scaled by 1/(Mx*My) so that the size-M correlation
 // carries the same Nx*Ny factor as the size-N one.
 static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spectrum) {
+    if (h->image_reuse && h->prepared_image == image_spectrum) return FASTFFT_OK;
+    h->prepared_image = nullptr;
     const int nx = (int)h->fwd_out.x, ny = (int)h->fwd_out.y;
     const int mx = (int)h->red_mx, my = (int)h->red_my;
     char* c = region_c(h);
@@ -729,7 +747,9 @@ static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spec
     // 4. forward along y at size My, scaled by 1/(Mx My): spec[kx][ky]
     ColArgs c4 = col_args(stage, my, my, spec, my, my, mx / 2 + 1);
     c4.out_scale = 1.f / ((float)mx * (float)my);
-    return stage_cols(h, my, ST_FWD, FASTFFT_DTYPE_C64, c4);
+    fastfft_status st4 = stage_cols(h, my, ST_FWD, FASTFFT_DTYPE_C64, c4);
+    if (st4 == FASTFFT_OK && h->image_reuse) h->prepared_image = image_spectrum;
+    return st4;
 }
 
 // Up to kMaxBatch templates through the reduced-size correlation against the prepared
@@ -815,15 +835,19 @@ fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const 
     if (!input || !image_spectrum) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null input or image pointer");
     fastfft_status st = xcorr_checks(h, pre_op, intra_op, post_op);
     if (st != FASTFFT_OK) return st;
-    return xcorr_one(h, input, image_spectrum, output ? output : const_cast<void*>(input), pre_op, intra_op, post_op);
+    void* out = output ? output : const_cast<void*>(input);
+    // With image reuse declared, a single template also goes through the reduced-size path:
+    // the image is prepared on the first call that names it and reused after that.
+    if (h->image_reuse && h->red_ok && !h->force_full_size)
+        return xcorr_many(h, 1, &input, nullptr, &image_spectrum, &out, pre_op, intra_op, post_op);
+    return xcorr_one(h, input, image_spectrum, out, pre_op, intra_op, post_op);
 }
 
 // Shared body of the batched calls; dims (x, y per template) may be NULL (plan size).
 static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inputs, const int* dims,
                                  const void* const* image_spectra, void* const* outputs, const fastfft_op* pre_op,
-                                 const fastfft_op* intra_op, const fastfft_op* post_op,
-                                 unsigned long long* peaks = nullptr, unsigned long long* mip = nullptr,
-                                 int mip_base = 0) {
+                                 const fastfft_op* intra_op, const fastfft_op* post_op, unsigned long long* peaks,
+                                 unsigned long long* mip, int mip_base) {
     // with a peak array or a projection the windows are written only where outputs[i] is set
     const bool reduce = peaks != nullptr || mip != nullptr;
     if (n < 0 || (n > 0 && (!inputs || !image_spectra)))

@@ -54,6 +54,12 @@ struct fastfft_plan_s {
     long long bytes_c = 0;     // prep work (max of the two column-major stages) + real crop + reduced spectrum
     long long off_c_real = 0, off_c_spec = 0;
     bool force_full_size = false;  // fastfft_set_full_size_correlation
+    // fastfft_set_image_reuse: the image spectrum at a given address is declared unchanged,
+    // so the reduced spectrum prepared for prepared_image (still in region C) is reused
+    // when the next call names the same address; cleared whenever region C may have been
+    // rewritten or the work moved to another stream.
+    bool image_reuse = false;
+    const void* prepared_image = nullptr;
     int red_batch = 8;              // templates per launch in the reduced-size path
     int red_batch_request = 8;      // fastfft_set_templates_per_launch (bounded by shared memory)
     long long red_t1_stride = 0, red_t2_stride = 0;  // complex elements per template slice

@@ -245,6 +245,13 @@ class FourierTransformer:
         self._check(self._lib.fastfft_templates_per_launch(self._h, ctypes.byref(v)))
         return v.value
 
+    def SetImageReuse(self, enable=True):
+        """Declare that image spectra do not change while in use: the reduced spectrum prepared
+        for an image address is reused by later calls naming the same address (single
+        FwdImageInvFFT calls then also correlate at the reduced size).  Calling it again, or
+        changing the plan or stream, forgets the prepared image."""
+        self._check(self._lib.fastfft_set_image_reuse(self._h, int(bool(enable))))
+
     def SetFullSizeCorrelation(self, force=True):
         """Make FwdImageInvFFTMany use the size-N kernels even when a smaller size is exact."""
         self._check(self._lib.fastfft_set_full_size_correlation(self._h, int(bool(force))))

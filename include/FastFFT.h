@@ -142,6 +142,8 @@ class FourierTransformer {
 
     // Extension: run on `stream` instead of cudaStreamPerThread.
     void SetStream(cudaStream_t stream) { check(fastfft_set_stream(h_, stream), "SetStream"); }
+    // Extension: declare that image spectra do not change while in use (fastfft_set_image_reuse).
+    void SetImageReuse(bool enable = true) { check(fastfft_set_image_reuse(h_, enable ? 1 : 0), "SetImageReuse"); }
 
     template <class PreOpType = std::nullptr_t, class IntraOpType = std::nullptr_t>
     void FwdFFT(InputType* input_ptr, InputType* output_ptr = nullptr, PreOpType pre_op = nullptr,

@@ -173,6 +173,15 @@ FASTFFT_API fastfft_status fastfft_templates_per_launch(fastfft_handle h, int* n
  * force != 0 selects the size-N kernels instead.  No reference counterpart (the
  * reference aborts on a forward increase with an inverse decrease, FastFFT.cu:673-679). */
 FASTFFT_API fastfft_status fastfft_set_full_size_correlation(fastfft_handle h, int force);
+
+/* enable != 0 declares that an image spectrum does not change while it is in use: the
+ * reduced spectrum prepared for an image address is then kept and reused by later calls
+ * naming the same address (batched or single FwdImageInvFFT, which then also correlates at
+ * the reduced size), instead of being prepared again in every call.  The caller must not
+ * modify the spectrum behind that address while reuse is on (or must call this again,
+ * which forgets the prepared image).  Changing the plan, the stream or the plan's settings
+ * also forgets it.  Default off.  No reference counterpart. */
+FASTFFT_API fastfft_status fastfft_set_image_reuse(fastfft_handle h, int enable);
 /* Transform size {x, y} that fastfft_fwd_image_inv_many uses for this plan. */
 FASTFFT_API fastfft_status fastfft_correlation_size(fastfft_handle h, int dims[2]);
 
