@@ -585,6 +585,35 @@ def run_ours(args, world, rank, local):
     if rank == 0 and not args.skip_uneven:
         uneven = [run_uneven(dev, images[0], "float32"), run_uneven(dev, images[0], "bfloat16")]
 
+    # ---- the reference's plain API: one FwdImageInvFFT call per template (rank 0) ----
+    plain = None
+    if rank == 0 and not args.skip_uneven:
+        plain = []
+        for reuse in (False, True):
+            single = F.FourierTransformer()
+            single.SetForwardFFTPlan(L, L, 1, N, N, 1)
+            single.SetInverseFFTPlan(N, N, 1, W, W, 1)
+            single.SetImageReuse(reuse)
+
+            def one_step(s_no):
+                for i in range(B):
+                    single.FwdImageInvFFT(ins[i], images[s_no % N_IMAGES], outs[i])
+
+            for s_no in range(2):
+                one_step(s_no)
+            torch.cuda.synchronize()
+            reps = 5
+            g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            g0.record()
+            for s_no in range(reps):
+                one_step(s_no)
+            g1.record()
+            torch.cuda.synchronize()
+            plain.append({"image_reuse": reuse, "value": reps * B / (g0.elapsed_time(g1) * 1e-3), "unit": UNIT,
+                          "correlation_size": list(single.CorrelationSize()) if reuse else [N, N],
+                          "how": "one FwdImageInvFFT call per template, " + str(B) + " per image, images rotating"})
+            del single
+
     # ---- the headline workload with FP16 / BF16 storage (rank 0) ----
     low = None
     low_checks = {}
@@ -667,7 +696,7 @@ def run_ours(args, world, rank, local):
             "clocks": clk,
             "cufft_pad_then_transform": cufft,
             "accuracy": accuracy,
-            "uneven_batch": uneven, "low_precision_storage": low,
+            "uneven_batch": uneven, "low_precision_storage": low, "plain_api": plain,
         }
         print(json.dumps(line), flush=True)
 

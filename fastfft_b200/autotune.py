@@ -13,7 +13,7 @@ from __future__ import annotations
 import json
 import os
 
-CANDIDATES = (4, 8, 16)
+CANDIDATES = (8, 16, 32, 64)
 
 
 def _key(ft, n_templates):

@@ -36,6 +36,9 @@ using namespace ffb;
 #define FFB_XCORR_TPB 8
 #endif
 
+// templates that one block of the fused column pass stages for a launch of n
+static inline int xcorr_tpb(int n) { return FFB_XCORR_TPB > 0 && n > FFB_XCORR_TPB ? FFB_XCORR_TPB : n; }
+
 // Lengths 3 * 2^k for the reduced-size correlation (1), or powers of two only (0).
 #ifndef FFB_ENABLE_FFT3
 #define FFB_ENABLE_FFT3 1
@@ -196,7 +199,8 @@ void size_buffers(fastfft_plan_s* h) {
             // templates per launch: bounded by the shared memory of the fused column kernel
             h->red_batch = h->red_batch_request;
             while (h->red_batch > 1 &&
-                   xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, h->red_batch) > 226 * 1024)
+                   xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, xcorr_tpb(h->red_batch)) >
+                       226 * 1024)
                 h->red_batch--;
             if (xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, 1) > 226 * 1024) {
                 h->red_ok = false;
@@ -792,11 +796,7 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const
     c.img = spec; c.img_stride = my;
     c.out = t2; c.out_pitch = h->pitch_b; c.out_batch = h->red_t2_stride; c.W = (int)h->inv_out.y;
     c.n_cols = mx / 2 + 1; c.n_batch = n;
-#if FFB_XCORR_TPB > 0
-    c.tpb = std::min(n, FFB_XCORR_TPB);
-#else
-    c.tpb = n;
-#endif
+    c.tpb = xcorr_tpb(n);
     if (dims)
         for (int g = 0; g < n; g++) c.L_g[g] = dims[2 * g + 1];
     c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
@@ -975,7 +975,8 @@ fastfft_status fastfft_fwd_image_inv_many_mip(fastfft_handle h, int n, const voi
 
 fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n) {
     if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
-    if (n < 1 || n > kMaxBatch) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "templates per launch must be in [1, 16]");
+    if (n < 1 || n > kMaxBatch)
+        return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "templates per launch must be in [1, " + std::to_string(kMaxBatch) + "]");
     h->red_batch_request = n;
     h->validated = false;
     if (h->fwd_set && h->inv_set) {

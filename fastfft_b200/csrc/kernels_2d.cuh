@@ -74,7 +74,10 @@ __device__ __forceinline__ int leading_slots(int L, int j) {
 // Row R2C (forward), two rows per complex FFT
 // ---------------------------------------------------------------------------
 // Templates per launch: blockIdx.y selects the template of a batch.
-constexpr int kMaxBatch = 16;
+// Templates per launch of the batched passes (grid.y).  Up to 64: more templates per launch
+// mean more blocks per launch and a shorter partly empty last wave in all three passes
+// (measured on B200 at 1536^2: 13.8, 12.1 and 11.5 us per template at 16, 32 and 64).
+constexpr int kMaxBatch = 64;
 
 struct RowFwdArgs {
     const void* in[kMaxBatch];  // real rows of template g: row r at in[g] + r * in_pitch (elements)

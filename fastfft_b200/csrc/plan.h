@@ -60,8 +60,8 @@ struct fastfft_plan_s {
     // rewritten or the work moved to another stream.
     bool image_reuse = false;
     const void* prepared_image = nullptr;
-    int red_batch = 8;              // templates per launch in the reduced-size path
-    int red_batch_request = 8;      // fastfft_set_templates_per_launch (bounded by shared memory)
+    int red_batch = 16;             // templates per launch in the reduced-size path
+    int red_batch_request = 16;     // fastfft_set_templates_per_launch (bounded by shared memory)
     long long red_t1_stride = 0, red_t2_stride = 0;  // complex elements per template slice
     long long off_c_t1 = 0, off_c_t2 = 0;
     int* dev_err = nullptr;  // device status word of bounded waits (inside the work buffer)

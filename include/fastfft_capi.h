@@ -160,7 +160,7 @@ FASTFFT_API fastfft_status fastfft_fwd_image_inv_many_mip(fastfft_handle h, int 
 /* Host-side decode of one peaks[] or mip[] entry. */
 FASTFFT_API void fastfft_decode_peak(unsigned long long key, float* value, unsigned int* index);
 
-/* Templates per launch of the batched reduced-size path (1..16, default 8; lowered if the
+/* Templates per launch of the batched reduced-size path (1..64, default 16; lowered if the
  * fused column kernel's shared memory would not fit), and the value in effect. */
 FASTFFT_API fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n);
 FASTFFT_API fastfft_status fastfft_templates_per_launch(fastfft_handle h, int* n);

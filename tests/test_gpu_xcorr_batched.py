@@ -194,3 +194,28 @@ def test_many_peaks_match_oracle_argmax(torch_cuda, write_windows, force_full):
             got = O.real_from_padded(host(outs[i]), iout)[0]
             assert O.rel_l2(got, ref) <= RTOL_L2_FP32
             assert O.peak(got)[0] == idx[i]
+
+
+def test_launches_beyond_sixteen_templates(torch_cuda):
+    """70 templates at 64 per launch (two launches, template slots past 16): windows and
+    fused peaks against the oracle."""
+    torch = torch_cuda
+    fin, fout, iout = (40, 40, 1), (512, 512, 1), (64, 64, 1)
+    ft = plan(fin, fout, iout)
+    ft.SetTemplatesPerLaunch(64)
+    assert ft.TemplatesPerLaunch() == 64
+    spec = O.image_spectrum_fp32(O.gaussian_blob_image(512, n_blobs=4, seed=23))
+    d_spec = dev(torch, spec.view(np.float32))
+    rng = np.random.default_rng(24)
+    ts = [rng.standard_normal((40, 40)).astype(np.float32) for _ in range(70)]
+    ins = [dev(torch, O.real_to_padded(t, fin)) for t in ts]
+    outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    peaks = torch.zeros(len(ts), dtype=torch.int64, device="cuda")
+    ft.FwdImageInvFFTManyPeaks(ins, d_spec, peaks, outputs=outs)
+    vals, idx = F.decode_peaks(peaks)
+    p = O.Plan(fin, fout, fout, iout)
+    for i in (0, 16, 17, 40, 63, 64, 69):
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(ts[i], fin), spec, p, out_dtype=np.float64), iout)
+        got = O.real_from_padded(host(outs[i]), iout)
+        assert O.rel_l2(got, ref) <= RTOL_L2_FP32, i
+        assert O.peak(got[0])[0] == idx[i], i
