@@ -1,7 +1,7 @@
 // Pass kernels at the lengths N = 3P of the reduced-size correlation (sm_100a).
 //
 // Same argument structures, data layouts and outputs as the power-of-two kernels in
-// kernels_2d.cuh / kernels_xcorr.cuh; only the FFT inside differs (BlockFft3, fft3.cuh):
+// kernels_2d.cuh / kernels_xcorr.cuh; only the FFT inside differs (length 3P, fft3.cuh):
 //   r2c3_rows_kernel   : row R2C, two real rows per complex FFT, transposed [kx][y] output
 //   c2r3_rows_kernel   : row C2R from [kx][y], two rows per complex FFT, fused peak search
 //   cols3_fwd_kernel   : forward column FFT (2D layout), zero padding y >= L, keep W
