@@ -39,6 +39,12 @@ using namespace ffb;
 // templates that one block of the fused column pass stages for a launch of n
 static inline int xcorr_tpb(int n) { return FFB_XCORR_TPB > 0 && n > FFB_XCORR_TPB ? FFB_XCORR_TPB : n; }
 
+// Uneven batches: each template correlates at its own exact size class (1), or every
+// template at the plan's size (0).
+#ifndef FFB_SIZE_CLASSES
+#define FFB_SIZE_CLASSES 1
+#endif
+
 // Lengths 3 * 2^k for the reduced-size correlation (1), or powers of two only (0).
 #ifndef FFB_ENABLE_FFT3
 #define FFB_ENABLE_FFT3 1
@@ -727,11 +733,11 @@ static fastfft_status xcorr_one(fastfft_handle h, const void* input, const void*
 // Prepare the reduced spectrum of one image: C2R of the size-N spectrum keeping
 // [0, My) x [0, Mx), R2C at size M, scaled by 1/(Mx*My) so that the size-M correlation
 // carries the same Nx*Ny factor as the size-N one.
-static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spectrum) {
-    if (h->image_reuse && h->prepared_image == image_spectrum) return FASTFFT_OK;
+static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spectrum, int mx, int my) {
+    if (h->image_reuse && h->prepared_image == image_spectrum && h->prepared_mx == mx && h->prepared_my == my)
+        return FASTFFT_OK;
     h->prepared_image = nullptr;
     const int nx = (int)h->fwd_out.x, ny = (int)h->fwd_out.y;
-    const int mx = (int)h->red_mx, my = (int)h->red_my;
     char* c = region_c(h);
     float2* stage = reinterpret_cast<float2*>(c);
     float* crop = reinterpret_cast<float*>(c + h->off_c_real);
@@ -752,18 +758,21 @@ static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spec
     ColArgs c4 = col_args(stage, my, my, spec, my, my, mx / 2 + 1);
     c4.out_scale = 1.f / ((float)mx * (float)my);
     fastfft_status st4 = stage_cols(h, my, ST_FWD, FASTFFT_DTYPE_C64, c4);
-    if (st4 == FASTFFT_OK && h->image_reuse) h->prepared_image = image_spectrum;
+    if (st4 == FASTFFT_OK && h->image_reuse) {
+        h->prepared_image = image_spectrum;
+        h->prepared_mx = mx;
+        h->prepared_my = my;
+    }
     return st4;
 }
 
 // Up to kMaxBatch templates through the reduced-size correlation against the prepared
 // spectrum: three launches whose grid.y runs over the templates.
-static fastfft_status red_xcorr_batch(fastfft_handle h, int n, const void* const* inputs, const int* dims,
-                                      void* const* outs, const fastfft_op* pre_op, const fastfft_op* intra_op,
-                                      const fastfft_op* post_op, unsigned long long* peaks = nullptr,
-                                      const int* slots = nullptr, unsigned long long* mip = nullptr,
-                                      int mip_base = 0) {
-    const int mx = (int)h->red_mx, my = (int)h->red_my;
+static fastfft_status red_xcorr_batch(fastfft_handle h, int mx, int my, int n, const void* const* inputs,
+                                      const int* dims, void* const* outs, const fastfft_op* pre_op,
+                                      const fastfft_op* intra_op, const fastfft_op* post_op,
+                                      unsigned long long* peaks = nullptr, const int* slots = nullptr,
+                                      unsigned long long* mip = nullptr, int mip_base = 0) {
     char* c0 = region_c(h);
     const float2* spec = reinterpret_cast<const float2*>(c0 + h->off_c_spec);
     float2* t1 = reinterpret_cast<float2*>(c0 + h->off_c_t1);
@@ -885,9 +894,22 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
         }
         return FASTFFT_OK;
     }
-    // Reduced-size path: templates are grouped by image (in order of first use); each
-    // distinct image is prepared once for the whole call; up to red_batch templates per launch.
+    // Reduced-size path: templates are grouped by image and, within an image, by size class
+    // (the exact correlation size of each template, which for templates smaller than the
+    // plan's can be smaller than the plan's), in order of first use; the image is prepared
+    // once per class for the whole call; up to red_batch templates per launch.
     std::vector<char> done(n, 0);
+    std::vector<int> cls_x(n), cls_y(n);
+    for (int k = 0; k < n; k++) {
+        cls_x[k] = (int)h->red_mx;
+        cls_y[k] = (int)h->red_my;
+#if FFB_SIZE_CLASSES
+        if (dims) {
+            cls_x[k] = (int)std::min<long long>(cls_x[k], corr_size_at_least(dims[2 * k] + h->inv_out.x - 1));
+            cls_y[k] = (int)std::min<long long>(cls_y[k], corr_size_at_least(dims[2 * k + 1] + h->inv_out.y - 1));
+        }
+#endif
+    }
     const void* grp_in[kMaxBatch];
     void* grp_out[kMaxBatch];
     int grp_dims[2 * kMaxBatch];
@@ -895,11 +917,12 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
     for (int i = 0; i < n; i++) {
         if (done[i]) continue;
         const void* img = image_spectra[i];
-        st = red_prepare_image(h, img);
+        const int mx = cls_x[i], my = cls_y[i];
+        st = red_prepare_image(h, img, mx, my);
         if (st != FASTFFT_OK) return st;
         int m = 0;
         for (int k = i; k < n; k++) {
-            if (done[k] || image_spectra[k] != img) continue;
+            if (done[k] || image_spectra[k] != img || cls_x[k] != mx || cls_y[k] != my) continue;
             grp_in[m] = inputs[k];
             grp_out[m] = reduce ? (outputs ? outputs[k] : nullptr)
                                 : ((outputs && outputs[k]) ? outputs[k] : const_cast<void*>(inputs[k]));
@@ -910,15 +933,15 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
             }
             done[k] = 1;
             if (++m == h->red_batch) {
-                st = red_xcorr_batch(h, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op, post_op,
-                                     peaks, grp_slot, mip, mip_base);
+                st = red_xcorr_batch(h, mx, my, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op,
+                                     post_op, peaks, grp_slot, mip, mip_base);
                 if (st != FASTFFT_OK) return st;
                 m = 0;
             }
         }
         if (m > 0) {
-            st = red_xcorr_batch(h, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op, post_op,
-                                 peaks, grp_slot, mip, mip_base);
+            st = red_xcorr_batch(h, mx, my, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op,
+                                 post_op, peaks, grp_slot, mip, mip_base);
             if (st != FASTFFT_OK) return st;
         }
     }

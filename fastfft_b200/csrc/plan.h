@@ -60,6 +60,7 @@ struct fastfft_plan_s {
     // rewritten or the work moved to another stream.
     bool image_reuse = false;
     const void* prepared_image = nullptr;
+    long long prepared_mx = 0, prepared_my = 0;   // the size it was prepared at
     int red_batch = 16;             // templates per launch in the reduced-size path
     int red_batch_request = 16;     // fastfft_set_templates_per_launch (bounded by shared memory)
     long long red_t1_stride = 0, red_t2_stride = 0;  // complex elements per template slice

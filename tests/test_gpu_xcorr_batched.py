@@ -219,3 +219,28 @@ def test_launches_beyond_sixteen_templates(torch_cuda):
         got = O.real_from_padded(host(outs[i]), iout)
         assert O.rel_l2(got, ref) <= RTOL_L2_FP32, i
         assert O.peak(got[0])[0] == idx[i], i
+
+
+def test_uneven_templates_use_their_own_size_class(torch_cuda):
+    """128^2 and 384^2 templates with 512^2 windows in one call: the 128s correlate at 768
+    (128 + 511 <= 768), the 384s at the plan's 1024; one image preparation per class."""
+    torch = torch_cuda
+    fmax, fout, iout = (384, 384, 1), (2048, 2048, 1), (512, 512, 1)
+    ft = plan(fmax, fout, iout)
+    assert ft.CorrelationSize() == (1024, 1024)
+    spec = image_spectrum(fout, 25)
+    d_spec = dev(torch, spec.view(np.float32))
+    rng = np.random.default_rng(26)
+    sizes = [(128, 128), (384, 384), (128, 128), (384, 384), (128, 128), (128, 128)]
+    ts = [rng.standard_normal((y, x)).astype(np.float32) for x, y in sizes]
+    ins = [dev(torch, O.real_to_padded(t, (x, y, 1))) for t, (x, y) in zip(ts, sizes)]
+    outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    before = ft.LaunchCount()
+    ft.FwdImageInvFFTManySized(ins, sizes, d_spec, outs)
+    assert ft.LaunchCount() - before == 2 * 4 + 2 * 3      # two preparations, one batch per class
+    for t, (x, y), o in zip(ts, sizes, outs):
+        p = O.Plan((x, y, 1), fout, fout, iout)
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, (x, y, 1)), spec, p, out_dtype=np.float64), iout)
+        got = O.real_from_padded(host(o), iout)
+        assert O.rel_l2(got, ref) <= RTOL_L2_FP32, (x, y)
+        assert O.rel_max(got, ref) <= RTOL_MAX_FP32, (x, y)
