@@ -122,13 +122,18 @@ fastfft_status validate(fastfft_plan_s* h) {
                 return fail(h, FASTFFT_ERR_INVALID_DIMS, "all dimensions must be <= 512 for 3d transforms");
     }
     if (dim != h->rank) return fail(h, FASTFFT_ERR_INVALID_DIMS, "plan dimensionality does not match the handle rank");
-    // powers of two (FastFFT.cu:895-927)
-    if ((!is_pow2(fi.x) || !is_pow2(fi.y) || !is_pow2(fi.z)) && h->fwd_change != SizeChange::Increase)
-        return fail(h, FASTFFT_ERR_INVALID_DIMS, "input dimensions must be powers of 2 unless the forward transform pads");
-    if (!is_pow2(fo.x) || !is_pow2(fo.y) || !is_pow2(fo.z))
-        return fail(h, FASTFFT_ERR_INVALID_DIMS, "forward output dimensions must be powers of 2");
-    if ((!is_pow2(io.x) || !is_pow2(io.y) || !is_pow2(io.z)) && h->inv_change != SizeChange::Decrease)
-        return fail(h, FASTFFT_ERR_INVALID_DIMS, "output dimensions must be powers of 2 unless the inverse transform crops");
+    // transform lengths: powers of two (FastFFT.cu:895-927); 2D plans also take 3 * 2^k with
+    // 128 <= 2^k <= 2048 (384 ... 6144), which the reference rejects
+    auto len_ok = [&](long long v) { return is_pow2(v) || (dim == 2 && v <= 6144 && ffb::is_3p_size((int)v)); };
+    const char* lens = dim == 2 ? "powers of 2 or 3 * 2^k (384 ... 6144)" : "powers of 2";
+    if ((!len_ok(fi.x) || !len_ok(fi.y) || !is_pow2(fi.z)) && h->fwd_change != SizeChange::Increase)
+        return fail(h, FASTFFT_ERR_INVALID_DIMS,
+                    std::string("input dimensions must be ") + lens + " unless the forward transform pads");
+    if (!len_ok(fo.x) || !len_ok(fo.y) || !is_pow2(fo.z))
+        return fail(h, FASTFFT_ERR_INVALID_DIMS, std::string("forward output dimensions must be ") + lens);
+    if ((!len_ok(io.x) || !len_ok(io.y) || !is_pow2(io.z)) && h->inv_change != SizeChange::Decrease)
+        return fail(h, FASTFFT_ERR_INVALID_DIMS,
+                    std::string("output dimensions must be ") + lens + " unless the inverse transform crops");
     // transform sizes handled by the block FFTs
     const long long nx = std::max(fi.x, fo.x), ny = std::max(fi.y, fo.y), nz = std::max(fi.z, fo.z);
     auto in_range = [](long long n) { return n >= ffb::kMinN && n <= ffb::kMaxN; };

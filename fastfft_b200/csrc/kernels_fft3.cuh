@@ -4,7 +4,7 @@
 // kernels_2d.cuh / kernels_xcorr.cuh; only the FFT inside differs (length 3P, fft3.cuh):
 //   r2c3_rows_kernel   : row R2C, two real rows per complex FFT, transposed [kx][y] output
 //   c2r3_rows_kernel   : row C2R from [kx][y], two rows per complex FFT, fused peak search
-//   cols3_fwd_kernel   : forward column FFT (2D layout), zero padding y >= L, keep W
+//   cols3_kernel       : column FFT (2D layout), forward / inverse / fused correlation, keep W
 //   xcorr3_cols_kernel : batched fused column pass (TMA-staged image and template columns,
 //                        forward, conj(T) * I, inverse), keep W
 // Time-domain data are loaded and stored in natural order; the spectrum side is decimated
@@ -207,12 +207,14 @@ c2r3_rows_kernel(RowInvArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Forward column FFT over the 2D [kx][y] layout (the image preparation of the
-// reduced-size correlation); general 3D addressing is not supported at these lengths.
+// Column passes over the 2D [kx][y] layout (modes as cols_kernel): FWD (the image
+// preparation of the reduced-size correlation and FwdFFT at these lengths), INV and the
+// single-template XCORR.  Output window [W0, W0 + W); the general 3D addressing of
+// cols_kernel is not supported at these lengths (3D transforms are powers of two).
 // ---------------------------------------------------------------------------
-template <int P, int FPB>
-__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB)
-cols3_fwd_kernel(ColArgs a) {
+template <int P, int MODE, class InC, class ImgC, int FPB>
+__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, (Fft3Shape<P>::T * FPB <= 256) ? 2 : 1)
+cols3_kernel(ColArgs a) {
     using S3 = Fft3Shape<P>;
     constexpr int T = S3::T;
     constexpr int TP = S3::TP;
@@ -226,26 +228,61 @@ cols3_fwd_kernel(ColArgs a) {
     const int col = blockIdx.x * FPB + f;
     const bool valid = col < a.n_cols;
     const long long bz = blockIdx.y;
-    const float2* pin = static_cast<const float2*>(a.in) + bz * a.in_batch_stride + (long long)col * a.in_stride;
-    auto ld = [&](int n) {
-        const float2 x = (valid && n < a.L) ? pin[n] : make_float2(0.f, 0.f);
-        return (a.in_scale != 1.f) ? cscale(x, a.in_scale) : x;
-    };
+    const InC* pin = static_cast<const InC*>(a.in) + bz * a.in_batch_stride + (long long)col * a.in_stride;
+    float2* pout = static_cast<float2*>(a.out) + bz * a.out_batch_stride + (long long)col * a.out_stride;
     float2 v[16];
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-        const int n1 = j + TP * q;
-        v[q] = dif_input<P>(ld(n1), ld(n1 + P), ld(n1 + 2 * P), n1, k2, a.tw3);
-    }
-    BlockFft<P, false>::run(v, g, j, a.tw, valid ? leading_slots3<P>(a.L, j) : 0);
-    if (valid) {
-        float2* pout = static_cast<float2*>(a.out) + bz * a.out_batch_stride + (long long)col * a.out_stride;
+    if constexpr (MODE == COL_INV) {
+        // spectrum X[k], k < L, natural order in the column: thread (k2, j) takes X[3 m + k2]
 #pragma unroll
         for (int q = 0; q < 16; q++) {
             const int k = 3 * (j + TP * q) + k2;
-            if (k < a.W) pout[k] = (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q];
+            const float2 x = (valid && k < a.L) ? ld_cplx<InC>(pin + k) : make_float2(0.f, 0.f);
+            v[q] = (a.in_scale != 1.f) ? cscale(x, a.in_scale) : x;
+        }
+        BlockFft<P, true>::run(v, g, j, a.tw, 16);
+    } else {
+        auto ld = [&](int n) {
+            const float2 x = (valid && n < a.L) ? ld_cplx<InC>(pin + n) : make_float2(0.f, 0.f);
+            return (a.in_scale != 1.f) ? cscale(x, a.in_scale) : x;
+        };
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int n1 = j + TP * q;
+            v[q] = dif_input<P>(ld(n1), ld(n1 + P), ld(n1 + 2 * P), n1, k2, a.tw3);
+        }
+        BlockFft<P, false>::run(v, g, j, a.tw, valid ? leading_slots3<P>(a.L, j) : 0);
+        if constexpr (MODE == COL_FWD) {
+            // spectrum side: X[3 m + k2] straight from the registers
+            if (valid) {
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    const int n = 3 * (j + TP * q) + k2 - a.W0;
+                    if (n >= 0 && n < a.W) pout[n] = (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q];
+                }
+            }
+            return;
+        } else {
+            if (a.intra_kind != 0) {
+                const ImgC* pimg =
+                    static_cast<const ImgC*>(a.img) + bz * a.img_batch_stride + (long long)col * a.img_stride;
+                const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    float2 im = make_float2(0.f, 0.f);
+                    if (valid) im = ld_cplx_stream<ImgC>(pimg + 3 * (j + TP * q) + k2);
+                    const float2 pr = conj_mul(v[q], im);
+                    v[q] = (sc != 1.f) ? cscale(pr, sc) : pr;
+                }
+            }
+            BlockFft<P, true>::run(v, g, j, a.tw, 16);
         }
     }
+    // INV and XCORR: radix-3 output pass, natural order
+    const int W = valid ? a.W : 0;
+    dit_output<P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
+        const int n = n0 - a.W0;
+        if (n >= 0 && n < W) pout[n] = (a.out_scale != 1.f) ? cscale(x, a.out_scale) : x;
+    });
 }
 
 // ---------------------------------------------------------------------------

@@ -25,11 +25,13 @@ cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream
 cudaError_t launch_xcorr_cols(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st);
 size_t xcorr_cols_smem(int n, int img_dtype, int L, int n_batch);
 
-// Lengths N = 3P (128 <= P <= 2048) of the reduced-size correlation; the public
-// launchers above forward them here (R2C, C2R, forward columns, fused columns only).
+// Lengths N = 3P (128 <= P <= 2048): the reduced-size correlation's internal sizes and the
+// 2D plans at these sizes; the public launchers above forward them here.
 cudaError_t launch_r2c3(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
 cudaError_t launch_c2r3(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
 cudaError_t launch_cols3_fwd(int n, const ColArgs& a, cudaStream_t st);
+cudaError_t launch_cols3_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st);
+cudaError_t launch_cols3_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_xcorr3(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st);
 size_t xcorr3_smem(int n, int img_dtype, int L, int n_batch);
 

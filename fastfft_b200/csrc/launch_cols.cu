@@ -47,9 +47,11 @@ cudaError_t launch_cols_fwd(int n, const ColArgs& a, cudaStream_t st) {
     FFB_SIZE_SWITCH(n, fwd_dispatch, a, st)
 }
 cudaError_t launch_cols_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st) {
+    if (is_3p_size(n)) return launch_cols3_inv(n, in_dtype, a, st);
     FFB_SIZE_SWITCH(n, inv_dispatch, in_dtype, a, st)
 }
 cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st) {
+    if (is_3p_size(n)) return launch_cols3_xcorr(n, img_dtype, a, st);
     FFB_SIZE_SWITCH(n, xcorr_dispatch, img_dtype, a, st)
 }
 

@@ -111,10 +111,10 @@ cudaError_t launch_c2r3(int n, int out_dtype, const RowInvArgs& a, cudaStream_t 
 }
 
 // ---------------------------------------------------------------------------
-template <int P>
-static cudaError_t cols3_fwd_impl(const ColArgs& a0, cudaStream_t st) {
-    // 2D layout only (the image preparation of the reduced-size correlation)
-    if (a0.in_div > 1 || a0.out_div > 1 || a0.out_elem_stride > 1 || a0.W0 != 0) return cudaErrorInvalidValue;
+template <int P, int MODE, class InC, class ImgC>
+static cudaError_t cols3_impl(const ColArgs& a0, cudaStream_t st) {
+    // 2D layout only (3D transforms are powers of two)
+    if (a0.in_div > 1 || a0.out_div > 1 || a0.out_elem_stride > 1) return cudaErrorInvalidValue;
     constexpr int FPB = col_fpb3<P>();
     constexpr int THREADS = Fft3Shape<P>::T * FPB;
     const size_t smem = (size_t)Fft3Group<P, FPB, true>::BYTES;
@@ -122,7 +122,7 @@ static cudaError_t cols3_fwd_impl(const ColArgs& a0, cudaStream_t st) {
     cudaError_t e = tables3(P, &a.tw, &a.tw3);
     if (e != cudaSuccess) return e;
     static std::atomic<unsigned long long> mask{0};
-    auto fn = cols3_fwd_kernel<P, FPB>;
+    auto fn = cols3_kernel<P, MODE, InC, ImgC, FPB>;
     if ((e = ensure_smem_attr((const void*)fn, smem, &mask)) != cudaSuccess) return e;
     const int grid = (a.n_cols + FPB - 1) / FPB;
     if (grid == 0) return cudaSuccess;
@@ -131,7 +131,36 @@ static cudaError_t cols3_fwd_impl(const ColArgs& a0, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_cols3_fwd(int n, const ColArgs& a, cudaStream_t st) { FFB_SIZE3_SWITCH(n, cols3_fwd_impl, a, st) }
+template <int P>
+static cudaError_t cols3_fwd_dispatch(const ColArgs& a, cudaStream_t st) {
+    return cols3_impl<P, COL_FWD, float2, float2>(a, st);
+}
+template <int P>
+static cudaError_t cols3_inv_dispatch(int in_dtype, const ColArgs& a, cudaStream_t st) {
+    switch (in_dtype) {
+        case 3: return cols3_impl<P, COL_INV, float2, float2>(a, st);
+        case 4: return cols3_impl<P, COL_INV, __half2, float2>(a, st);
+        case 5: return cols3_impl<P, COL_INV, __nv_bfloat162, float2>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <int P>
+static cudaError_t cols3_xcorr_dispatch(int img_dtype, const ColArgs& a, cudaStream_t st) {
+    switch (img_dtype) {
+        case 3: return cols3_impl<P, COL_XCORR, float2, float2>(a, st);
+        case 4: return cols3_impl<P, COL_XCORR, float2, __half2>(a, st);
+        case 5: return cols3_impl<P, COL_XCORR, float2, __nv_bfloat162>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_cols3_fwd(int n, const ColArgs& a, cudaStream_t st) { FFB_SIZE3_SWITCH(n, cols3_fwd_dispatch, a, st) }
+cudaError_t launch_cols3_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st) {
+    FFB_SIZE3_SWITCH(n, cols3_inv_dispatch, in_dtype, a, st)
+}
+cudaError_t launch_cols3_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st) {
+    FFB_SIZE3_SWITCH(n, cols3_xcorr_dispatch, img_dtype, a, st)
+}
 
 // ---------------------------------------------------------------------------
 // dynamic shared memory available to one block (227 KB, less a little static shared memory)

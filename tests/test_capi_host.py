@@ -64,7 +64,9 @@ def test_memory_sizes_match_reference(fin, fout, iout):
     ((64, 64, 1), (512, 512, 1), (256, 256, 1), (256, 256, 1), C.ERR_INVALID_DIMS),  # fwd out != inv in
     ((64, 128, 1), (128, 64, 1), (128, 64, 1), (128, 64, 1), C.ERR_INVALID_DIMS),    # mixed grow/shrink
     ((100, 100, 1), (100, 100, 1), (100, 100, 1), (100, 100, 1), C.ERR_INVALID_DIMS),  # non-pow2, no pad
-    ((64, 64, 1), (384, 384, 1), (384, 384, 1), (384, 384, 1), C.ERR_INVALID_DIMS),  # non-pow2 fwd out
+    ((64, 64, 1), (320, 320, 1), (320, 320, 1), (320, 320, 1), C.ERR_INVALID_DIMS),  # 5 * 2^k fwd out
+    ((64, 64, 1), (192, 192, 1), (192, 192, 1), (192, 192, 1), C.ERR_INVALID_DIMS),  # 3 * 2^k below 384
+    ((16, 16, 16), (384, 384, 384), (384, 384, 384), (384, 384, 384), C.ERR_INVALID_DIMS),  # 3 * 2^k in 3D
     ((64, 64, 1), (512, 512, 1), (512, 512, 1), (600, 600, 1), C.ERR_INVALID_DIMS),  # inverse grows, non-pow2
     ((64, 64, 64), (1024, 1024, 1024), (1024, 1024, 1024), (1024, 1024, 1024), C.ERR_INVALID_DIMS),  # 3D > 512
     ((64, 64, 1), (16384, 16384, 1), (16384, 16384, 1), (16384, 16384, 1), C.ERR_UNSUPPORTED),  # > 8192
@@ -76,6 +78,19 @@ def test_validation_rejects(fin, fout, iin, iout, status):
     with pytest.raises(F.FastFFTError) as e:
         ft.SetInverseFFTPlan(*iin, *iout)
     assert e.value.status == status
+
+
+@pytest.mark.parametrize("fin,fout,iout", [
+    ((64, 64, 1), (384, 384, 1), (384, 384, 1)),
+    ((1536, 1536, 1), (1536, 1536, 1), (700, 600, 1)),
+    ((100, 200, 1), (768, 6144, 1), (768, 6144, 1)),
+    ((1000, 10, 1), (3072, 32, 1), (3000, 20, 1)),
+])
+def test_three_times_power_of_two_lengths_accepted_in_2d(fin, fout, iout):
+    ft = new()
+    ft.SetForwardFFTPlan(*fin, *fout)
+    ft.SetInverseFFTPlan(*fout, *iout)
+    assert ft.ReturnFwdOutputDimensions()[:3] == fout
 
 
 def test_rank_mismatch_rejected():
