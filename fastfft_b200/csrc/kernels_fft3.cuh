@@ -98,7 +98,9 @@ r2c3_rows_kernel(RowFwdArgs a) {
 #define FFB_C2R3_MIN_BLOCKS 3
 #endif
 
-template <int P, class OutT, int FPB>
+// PLAIN: windows written at origin 0, no peak search, no projection (the epilogue is then
+// only the bounds check and the stores).
+template <int P, class OutT, int FPB, bool PLAIN>
 __global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, FFB_C2R3_MIN_BLOCKS)
 c2r3_rows_kernel(RowInvArgs a) {
     using S3 = Fft3Shape<P>;
@@ -108,9 +110,8 @@ c2r3_rows_kernel(RowInvArgs a) {
     constexpr int H = N / 2;
     extern __shared__ float2 smem[];
     using G = Fft3Group<P, FPB, false, S3::SUB_C2R>;
-    // Z[k] of FFT ff at sf[dec(k)]: decimated by 3, so that sub-FFT k2 finds its inputs
-    // Z[3 m + k2] contiguous in its own region
-    auto dec = [](int k) { return (k % 3) * G::SUB + phys(k / 3); };
+    // Z[k] of FFT ff goes to region k % 3 at phys(k / 3) (decimated by 3, so that sub-FFT k2
+    // finds its inputs Z[3 m + k2] contiguous in its own region)
     const int f = threadIdx.x / T;
     const int t = threadIdx.x - f * T;
     const int k2 = t / TP;
@@ -138,19 +139,26 @@ c2r3_rows_kernel(RowInvArgs a) {
             }
         }
     }
+    // Item it of this thread has k = k0 + T it and T = 3 T': k % 3 and (N - k) % 3 stay fixed
+    // and k / 3 moves by T' per item, so the divisions by 3 are done once.
+    const int ff0 = threadIdx.x % FPB;
+    const int k0 = threadIdx.x / FPB;
+    float2* const sf = smem + ff0 * G::STRIDE;
+    const int kq0 = k0 / 3, kr0 = k0 - 3 * (k0 / 3);
+    const int nq0 = (N - k0) / 3, nr0 = (N - k0) - 3 * ((N - k0) / 3);
+    float2* const s_k = sf + kr0 * G::SUB;
+    float2* const s_nk = sf + nr0 * G::SUB;
+    static_assert((T * FPB) % FPB == 0 && T % 3 == 0, "item stride");
 #pragma unroll
     for (int it = 0; it < kItemsPerThread; it++) {
-        const int i = threadIdx.x + it * (T * FPB);
-        if (i < items) {
-            const int ff = i % FPB;
-            const int k = i / FPB;
+        const int k = k0 + T * it;
+        if (k <= H) {
             const float2 A = make_float2(ld[it].x, ld[it].y), B = make_float2(ld[it].z, ld[it].w);
-            float2* sf = smem + ff * G::STRIDE;
             if (k == 0 || k == H) {
-                sf[dec(k)] = make_float2(A.x, B.x);
+                s_k[phys(kq0 + TP * it)] = make_float2(A.x, B.x);
             } else {
-                sf[dec(k)] = make_float2(A.x - B.y, A.y + B.x);
-                sf[dec(N - k)] = make_float2(A.x + B.y, B.x - A.y);
+                s_k[phys(kq0 + TP * it)] = make_float2(A.x - B.y, A.y + B.x);
+                s_nk[phys(nq0 - TP * it)] = make_float2(A.x + B.y, B.x - A.y);
             }
         }
     }
@@ -168,41 +176,51 @@ c2r3_rows_kernel(RowInvArgs a) {
     OutT* oa = static_cast<OutT*>(a.out[blockIdx.y]) + (long long)ra * a.out_pitch;
     OutT* ob = oa + a.out_pitch;
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
-    const bool write = !a.peaks_only;
-    unsigned long long best = 0;
-    const unsigned int tmpl = (unsigned)(a.mip_base + a.peak_slot[blockIdx.y]);
-    unsigned long long* ma = a.mip ? a.mip + (long long)ra * a.W : nullptr;
-    dit_output<P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
-        const int n = n0 - a.X0;
-        if (n >= 0 && n < a.W) {
-            const float va = x.x * a.scale, vb = x.y * a.scale;
-            if (write) {
-                if (has_a) st_real<OutT>(oa + n, va);
-                if (has_b) st_real<OutT>(ob + n, vb);
+    if constexpr (PLAIN) {
+        dit_output<P>(v, g, j, t, a.tw3, [&](int n, float2 x) {
+            if (n < a.W) {
+                if (has_a) st_real<OutT>(oa + n, x.x * a.scale);
+                if (has_b) st_real<OutT>(ob + n, x.y * a.scale);
             }
-            if (ma) {
-                if (has_a) atomicMax(ma + n, peak_key(va, tmpl));
-                if (has_b) atomicMax(ma + a.W + n, peak_key(vb, tmpl));
-            }
-            if (a.peaks) {
-                if (has_a) {
-                    const unsigned long long k = peak_key(va, (unsigned)(ra * a.W + n));
-                    best = k > best ? k : best;
+        });
+        return;
+    } else {
+        const bool write = !a.peaks_only;
+        unsigned long long best = 0;
+        const unsigned int tmpl = (unsigned)(a.mip_base + a.peak_slot[blockIdx.y]);
+        unsigned long long* ma = a.mip ? a.mip + (long long)ra * a.W : nullptr;
+        dit_output<P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
+            const int n = n0 - a.X0;
+            if (n >= 0 && n < a.W) {
+                const float va = x.x * a.scale, vb = x.y * a.scale;
+                if (write) {
+                    if (has_a) st_real<OutT>(oa + n, va);
+                    if (has_b) st_real<OutT>(ob + n, vb);
                 }
-                if (has_b) {
-                    const unsigned long long k = peak_key(vb, (unsigned)((ra + 1) * a.W + n));
-                    best = k > best ? k : best;
+                if (ma) {
+                    if (has_a) atomicMax(ma + n, peak_key(va, tmpl));
+                    if (has_b) atomicMax(ma + a.W + n, peak_key(vb, tmpl));
+                }
+                if (a.peaks) {
+                    if (has_a) {
+                        const unsigned long long k = peak_key(va, (unsigned)(ra * a.W + n));
+                        best = k > best ? k : best;
+                    }
+                    if (has_b) {
+                        const unsigned long long k = peak_key(vb, (unsigned)((ra + 1) * a.W + n));
+                        best = k > best ? k : best;
+                    }
                 }
             }
-        }
-    });
-    if (a.peaks) {
+        });
+        if (a.peaks) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
-            best = other > best ? other : best;
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+                best = other > best ? other : best;
+            }
+            if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(a.peaks + a.peak_slot[blockIdx.y], best);
         }
-        if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(a.peaks + a.peak_slot[blockIdx.y], best);
     }
 }
 

@@ -4,6 +4,7 @@
 #include "kernels_fft3.cuh"
 #include "launch_common.cuh"
 
+
 namespace ffb {
 
 #define FFB_SIZE3_SWITCH(n, FN, ...)                 \
@@ -86,9 +87,11 @@ static cudaError_t c2r3_impl(const RowInvArgs& a0, cudaStream_t st) {
     RowInvArgs a = a0;
     cudaError_t e = tables3(P, &a.tw, &a.tw3);
     if (e != cudaSuccess) return e;
-    static std::atomic<unsigned long long> mask{0};
-    auto fn = c2r3_rows_kernel<P, OutT, FPB>;
-    if ((e = ensure_smem_attr((const void*)fn, smem, &mask)) != cudaSuccess) return e;
+    static std::atomic<unsigned long long> mask_plain{0}, mask_full{0};
+    // plain windows (no peak search, no projection, origin 0): the short epilogue
+    const bool plain = !a.peaks && !a.mip && !a.peaks_only && a.X0 == 0;
+    auto fn = plain ? c2r3_rows_kernel<P, OutT, FPB, true> : c2r3_rows_kernel<P, OutT, FPB, false>;
+    if ((e = ensure_smem_attr((const void*)fn, smem, plain ? &mask_plain : &mask_full)) != cudaSuccess) return e;
     const int grid = (a.n_rows + 2 * FPB - 1) / (2 * FPB);
     if (grid == 0) return cudaSuccess;
     if (a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
