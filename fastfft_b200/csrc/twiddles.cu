@@ -11,31 +11,40 @@ namespace ffb {
 static __global__ void init_twiddles_kernel(float2* tw) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= kTwTotal) return;
-    // locate (size n, pass stride ns, r, t) of entry gid
+    // locate (size n, pass, r, t) of entry gid; layout in FftShape
     int base = 0;
     for (int n = kMinN; n <= kMaxN; n *= 2) {
         const int sz = tw_size_of(n);
         if (gid < base + sz) {
             int local = gid - base;
             const int log = ilog2(n);
-            int ns = 1 << (log & 3);
+            const int rem = 1 << (log & 3);
             const int np16 = log >> 2;
-            for (int p = 0; p < np16; p++) {
-                if (ns > 1) {
-                    if (local < 16 * ns) {
-                        const int r = local / ns;
-                        const int t = local - r * ns;
-                        // exp(-2 pi i r t / (16 ns)) = cospi(-x) + i sinpi(-x), x = r t / (8 ns)
-                        const double x = -(double)(r * t) / (double)(8 * ns);
-                        double sv, cv;
-                        sincospi(x, &sv, &cv);
-                        tw[gid] = make_float2((float)cv, (float)sv);
-                        return;
-                    }
-                    local -= 16 * ns;
+            // exponent e of W_d^e = exp(-2 pi i e / d) = cospi(-x) + i sinpi(-x), x = 2 e / d
+            long long e = 0, d = 1;
+            int ns = 16;
+            int p = 1;
+            for (; p < np16; p++) {
+                if (local < 16 * ns) {
+                    const int r = local / ns;
+                    e = (long long)r * (local - r * ns);
+                    d = 16LL * ns;
+                    break;
                 }
+                local -= 16 * ns;
                 ns *= 16;
             }
+            if (p == np16) {
+                // closing radix-rem pass: (r-1) n/rem + b  ->  W_n^(r b)
+                const int nr = n / rem;
+                const int r = 1 + local / nr;
+                e = (long long)r * (local - (r - 1) * nr);
+                d = n;
+            }
+            const double x = -2.0 * (double)e / (double)d;
+            double sv, cv;
+            sincospi(x, &sv, &cv);
+            tw[gid] = make_float2((float)cv, (float)sv);
             return;
         }
         base += sz;
