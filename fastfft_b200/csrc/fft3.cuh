@@ -51,10 +51,15 @@ struct Fft3Shape {
     static constexpr int TP = P / 16;                  // threads per sub-FFT
     static constexpr int T = 3 * TP;                   // threads per FFT
     static constexpr int SUB = FftShape<P>::SMEM_PAD;  // float2 per sub-FFT region
-    // Region stride of the row C2R, which writes its input spectrum decimated by 3 (Z[k] in
-    // region k % 3 at phys(k / 3)): 5 past a multiple of 16 keeps both that scatter and the
-    // sub-FFTs' unit-stride loads within one or two shared-memory wavefronts per access.
-    static constexpr int SUB_C2R = (FftShape<P>::SMEM + 15) / 16 * 16 + 5;
+    // Region and FFT strides of the row C2R, which writes its input spectrum decimated by 3
+    // (Z[k] of FFT ff in region k % 3 at phys(k / 3)); a warp's scatter covers 8 consecutive
+    // k of each of 4 FFTs (P = 512; 2..16 FFTs per block at the other sizes).  The offsets past
+    // a multiple of 16 are the ones a bank model of that scatter finds best for the block
+    // shape of each P (at P = 512: 400 instead of 768 wavefronts per block); the sub-FFT
+    // exchanges read and write within one region and are conflict-free for any offset.
+    static constexpr int C2R_SUB_EXTRA = P == 128 ? 5 : P == 256 ? 1 : P == 512 ? 3 : P == 1024 ? 3 : 11;
+    static constexpr int C2R_FFT_EXTRA = P == 128 ? 0 : P == 256 ? 3 : P == 512 ? 3 : P == 1024 ? 15 : 0;
+    static constexpr int SUB_C2R = (FftShape<P>::SMEM + 15) / 16 * 16 + C2R_SUB_EXTRA;
     static constexpr int SMEM = 3 * SUB;               // float2 per exchange buffer
     static constexpr int ROUNDS = (P + T - 1) / T;     // radix-3 items per thread (6)
 };
@@ -76,7 +81,7 @@ __device__ __forceinline__ int loc3(int k) {
 // Every buffer that the radix-3 step reads across regions is rewritten only after a
 // sync_fft() that all its readers passed (the kernels call sync_fft() where a sub-FFT
 // exchange follows such reads).  Double buffering (DB) as in FftGroup.
-template <int P, int FPB, bool DB, int SUBX = Fft3Shape<P>::SUB>
+template <int P, int FPB, bool DB, int SUBX = Fft3Shape<P>::SUB, int PADX = 0>
 struct Fft3Group {
     using S3 = Fft3Shape<P>;
     static constexpr int T = S3::T;
@@ -84,7 +89,7 @@ struct Fft3Group {
     static_assert(SUBX >= FftShape<P>::SMEM, "a region must hold one sub-FFT's exchange");
     static constexpr int SUB = SUBX;                  // region stride (float2)
     static constexpr int SMEM = 3 * SUBX;             // float2 per exchange buffer
-    static constexpr int STRIDE = (DB ? 2 : 1) * SMEM;
+    static constexpr int STRIDE = (DB ? 2 : 1) * SMEM + PADX;  // float2 per FFT
     static constexpr int BYTES = FPB * STRIDE * (int)sizeof(float2);
     static_assert(TP <= 32 || 4 * FPB <= 15, "named barriers: FFT ids 1..FPB, sub-FFT ids FPB+1..4 FPB");
     float2* base;

@@ -109,7 +109,7 @@ c2r3_rows_kernel(RowInvArgs a) {
     constexpr int TP = S3::TP;
     constexpr int H = N / 2;
     extern __shared__ float2 smem[];
-    using G = Fft3Group<P, FPB, false, S3::SUB_C2R>;
+    using G = Fft3Group<P, FPB, false, S3::SUB_C2R, S3::C2R_FFT_EXTRA>;
     // Z[k] of FFT ff goes to region k % 3 at phys(k / 3) (decimated by 3, so that sub-FFT k2
     // finds its inputs Z[3 m + k2] contiguous in its own region)
     const int f = threadIdx.x / T;
@@ -326,12 +326,15 @@ struct Xcorr3Smem {
     static __host__ __device__ constexpr int total(int L, int nb) { return bar_off(L, nb) + 16; }
 };
 
-#ifndef FFB_XCORR3_MIN_BLOCKS
-#define FFB_XCORR3_MIN_BLOCKS 2
-#endif
+// Resident threads per SM the register budget is sized for: 384 (168 registers), as 4 blocks
+// of one 1536-point FFT (96 threads) each.  Small blocks beat 2 blocks of 2 FFTs (named
+// barriers per FFT) on B200: 5.66 instead of 5.94 us per template at 1536 points, 1.41
+// instead of 1.58 at 768; a budget of 576 threads (96 registers) spills and loses at 1536.
+constexpr int kXcorr3SmThreads = 384;
 
 template <int P, class ImgC, int FPB, bool MUL>
-__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, (Fft3Shape<P>::T * FPB <= 256) ? FFB_XCORR3_MIN_BLOCKS : 1)
+__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB,
+                                  Fft3Shape<P>::T * FPB < kXcorr3SmThreads ? kXcorr3SmThreads / (Fft3Shape<P>::T * FPB) : 1)
 xcorr3_cols_kernel(XcorrColArgs a) {
     using S3 = Fft3Shape<P>;
     using SM = Xcorr3Smem<P, ImgC, FPB>;
@@ -403,10 +406,16 @@ xcorr3_cols_kernel(XcorrColArgs a) {
         }
         BlockFft<P, false>::run(v, grp, j, a.tw, live ? leading_slots3<P>(Lg, j) : 0);
         if constexpr (MUL) {
+            // CONJ_MUL (scale 1) skips the 32 multiplies of the scaling
+            if (sc == 1.f) {
 #pragma unroll
-            for (int q = 0; q < 16; q++) {
-                const float2 im = lds_cplx<ImgC>(img_s + 3 * (j + TP * q) + k2);
-                v[q] = cscale(conj_mul(v[q], im), sc);
+                for (int q = 0; q < 16; q++) v[q] = conj_mul(v[q], lds_cplx<ImgC>(img_s + 3 * (j + TP * q) + k2));
+            } else {
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    const float2 im = lds_cplx<ImgC>(img_s + 3 * (j + TP * q) + k2);
+                    v[q] = cscale(conj_mul(v[q], im), sc);
+                }
             }
         }
         BlockFft<P, true>::run(v, grp, j, a.tw, 16);

@@ -138,10 +138,13 @@ xcorr_cols_kernel(XcorrColArgs a) {
         }
         BlockFft<N, false>::run(v, grp, j, a.tw, live ? leading_slots<T>(Lg, j) : 0);
         if constexpr (MUL) {
+            // CONJ_MUL (scale 1) skips the 32 multiplies of the scaling
+            if (sc == 1.f) {
 #pragma unroll
-            for (int q = 0; q < 16; q++) {
-                const float2 im = lds_cplx<ImgC>(img_s + j + T * q);
-                v[q] = cscale(conj_mul(v[q], im), sc);
+                for (int q = 0; q < 16; q++) v[q] = conj_mul(v[q], lds_cplx<ImgC>(img_s + j + T * q));
+            } else {
+#pragma unroll
+                for (int q = 0; q < 16; q++) v[q] = cscale(conj_mul(v[q], lds_cplx<ImgC>(img_s + j + T * q)), sc);
             }
         }
         BlockFft<N, true>::run(v, grp, j, a.tw, 16);

@@ -36,6 +36,12 @@ template <int P>
 constexpr int col_fpb3() {
     return fpb3_for(Fft3Shape<P>::T, 256);
 }
+// batched fused column pass: blocks of about 96 threads (one FFT from P = 512 up; 2 and 4
+// FFTs of 48 and 24 threads below)
+template <int P>
+constexpr int xcorr3_fpb() {
+    return fpb3_for(Fft3Shape<P>::T, 96);
+}
 static_assert(Fft3Shape<128>::T * row_fpb3<128>() % 32 == 0 && Fft3Shape<128>::T * col_fpb3<128>() % 32 == 0, "warps");
 static_assert(Fft3Shape<256>::T * row_fpb3<256>() % 32 == 0 && Fft3Shape<256>::T * col_fpb3<256>() % 32 == 0, "warps");
 
@@ -83,7 +89,7 @@ template <int P, class OutT>
 static cudaError_t c2r3_impl(const RowInvArgs& a0, cudaStream_t st) {
     constexpr int FPB = row_fpb3<P>();
     constexpr int THREADS = Fft3Shape<P>::T * FPB;
-    const size_t smem = (size_t)Fft3Group<P, FPB, false, Fft3Shape<P>::SUB_C2R>::BYTES;
+    const size_t smem = (size_t)Fft3Group<P, FPB, false, Fft3Shape<P>::SUB_C2R, Fft3Shape<P>::C2R_FFT_EXTRA>::BYTES;
     RowInvArgs a = a0;
     cudaError_t e = tables3(P, &a.tw, &a.tw3);
     if (e != cudaSuccess) return e;
@@ -171,7 +177,7 @@ constexpr int kMaxDynSmem3 = 227 * 1024 - 1024;
 
 template <int P, class ImgC>
 static cudaError_t xcorr3_impl(const XcorrColArgs& a0, cudaStream_t st) {
-    constexpr int FPB = col_fpb3<P>();
+    constexpr int FPB = xcorr3_fpb<P>();
     using SM = Xcorr3Smem<P, ImgC, FPB>;
     if (a0.n_batch < 1 || a0.n_batch > kMaxBatch || a0.n_cols < 1) return cudaErrorInvalidValue;
     if (a0.tpb < 1 || a0.tpb > a0.n_batch) return cudaErrorInvalidValue;
@@ -204,7 +210,7 @@ cudaError_t launch_xcorr3(int n, int img_dtype, const XcorrColArgs& a, cudaStrea
 
 template <int P>
 static size_t xcorr3_smem_p(int img_dtype, int L, int n_batch) {
-    constexpr int FPB = col_fpb3<P>();
+    constexpr int FPB = xcorr3_fpb<P>();
     if (img_dtype == 3) return (size_t)Xcorr3Smem<P, float2, FPB>::total(L, n_batch);
     return (size_t)Xcorr3Smem<P, __half2, FPB>::total(L, n_batch);
 }
