@@ -181,8 +181,9 @@ __device__ __forceinline__ void dit_output(float2 (&v)[16], G& g, int j, int t, 
         if (n1 < P) {
             const int p = phys(n1);
             float2 a = buf[p];
-            float2 b = cmulc(buf[G::SUB + p], ld_tw(tw3 + n1));
-            float2 c = cmulc(buf[2 * G::SUB + p], ld_tw(tw3 + 2 * n1));
+            const float2 w1 = ld_tw(tw3 + n1), w2 = cmul(w1, w1);  // one load: W^2n1 = (W^n1)^2
+            float2 b = cmulc(buf[G::SUB + p], w1);
+            float2 c = cmulc(buf[2 * G::SUB + p], w2);
             idft3(a, b, c);
             store(n1, a);
             store(n1 + P, b);
@@ -215,8 +216,9 @@ __device__ __forceinline__ float2* forward_dit(float2 (&v)[16], G& g, int j, int
         if (k1 < P) {
             const int p = phys(k1);
             const float2 a = buf[p];
-            const float2 b = cmul(buf[G::SUB + p], ld_tw(tw3 + k1));
-            const float2 c = cmul(buf[2 * G::SUB + p], ld_tw(tw3 + 2 * k1));
+            const float2 w1 = ld_tw(tw3 + k1), w2 = cmul(w1, w1);
+            const float2 b = cmul(buf[G::SUB + p], w1);
+            const float2 c = cmul(buf[2 * G::SUB + p], w2);
             buf[p] = dft3_component(a, b, c, 0);
             buf[G::SUB + p] = dft3_component(a, b, c, 1);
             buf[2 * G::SUB + p] = dft3_component(a, b, c, 2);

@@ -115,6 +115,29 @@ __device__ __forceinline__ float2 mul_w16(float2 a) {
     }
 }
 
+// mul_w16 with the exponent known after unrolling
+template <bool INV>
+__device__ __forceinline__ float2 mul_w16_k(float2 a, int m) {
+    switch (m & 15) {
+        case 1: return mul_w16<INV, 1>(a);
+        case 2: return mul_w16<INV, 2>(a);
+        case 3: return mul_w16<INV, 3>(a);
+        case 4: return mul_w16<INV, 4>(a);
+        case 5: return mul_w16<INV, 5>(a);
+        case 6: return mul_w16<INV, 6>(a);
+        case 7: return mul_w16<INV, 7>(a);
+        case 8: return mul_w16<INV, 8>(a);
+        case 9: return mul_w16<INV, 9>(a);
+        case 10: return mul_w16<INV, 10>(a);
+        case 11: return mul_w16<INV, 11>(a);
+        case 12: return mul_w16<INV, 12>(a);
+        case 13: return mul_w16<INV, 13>(a);
+        case 14: return mul_w16<INV, 14>(a);
+        case 15: return mul_w16<INV, 15>(a);
+        default: return a;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Small DFTs on registers (natural order in, natural order out)
 // ---------------------------------------------------------------------------
@@ -421,12 +444,18 @@ struct BlockFft {
             constexpr int R = S::REM;
             constexpr int M = 16 / R;
             const float2* __restrict__ t = tw + S::TW_REM;
+            // W_N^(r (j + T m)) = W_N^(r j) W_16^(r m): R-1 loads, the rest are constant turns
+            // (fewer L1 wavefronts, the binding unit of the row passes; measured on B200:
+            // C2R 2.97 instead of 3.10 us per template at 1536 points)
+            float2 wj[R];
+#pragma unroll
+            for (int r = 1; r < R; r++) wj[r] = ld_tw(t + (r - 1) * (N / R) + j);
 #pragma unroll
             for (int m = 0; m < M; m++) {
 #pragma unroll
                 for (int r = 1; r < R; r++) {
-                    const float2 w = ld_tw(t + (r - 1) * (N / R) + j + T * m);
-                    v[m + r * M] = INV ? cmulc(v[m + r * M], w) : cmul(v[m + r * M], w);
+                    const float2 x = mul_w16_k<INV>(v[m + r * M], r * m);
+                    v[m + r * M] = INV ? cmulc(x, wj[r]) : cmul(x, wj[r]);
                 }
             }
             radix_pass<R, M>(v);
