@@ -227,8 +227,35 @@ void size_buffers(fastfft_plan_s* h) {
     }
 }
 
+// Side stream and events of the image preparation (created once, outside any stream
+// capture since allocate() runs before a plan's first launch; left null on failure).
+static void create_prep_stream(fastfft_plan_s* h) {
+    if (h->prep_stream || !h->red_ok) return;
+    int dev = 0, lo = 0, hi = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    cudaStream_t s = nullptr;
+    cudaEvent_t f = nullptr, j = nullptr;
+    if (cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&j, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (j) cudaEventDestroy(j);
+        if (f) cudaEventDestroy(f);
+        if (s) cudaStreamDestroy(s);
+        return;
+    }
+    h->prep_stream = s;
+    h->prep_fork = f;
+    h->prep_join = j;
+    h->prep_device = dev;
+}
+
 fastfft_status allocate(fastfft_plan_s* h) {
     size_buffers(h);
+    create_prep_stream(h);
     const size_t need = (size_t)(h->bytes_a + h->bytes_b + h->bytes_c) + 256;
     if (h->buffer && h->buffer_bytes >= need) return FASTFFT_OK;
     if (h->buffer) {
@@ -564,6 +591,12 @@ fastfft_status fastfft_create(fastfft_handle* out, int compute_dtype, int input_
 
 fastfft_status fastfft_destroy(fastfft_handle h) {
     if (!h) return FASTFFT_OK;
+    if (h->prep_stream) {
+        cudaStreamSynchronize(h->prep_stream);
+        cudaEventDestroy(h->prep_fork);
+        cudaEventDestroy(h->prep_join);
+        cudaStreamDestroy(h->prep_stream);
+    }
     if (h->buffer) {
         cudaStreamSynchronize(h->stream);
         cudaFree(h->buffer);
@@ -738,9 +771,44 @@ static fastfft_status xcorr_one(fastfft_handle h, const void* input, const void*
 // Prepare the reduced spectrum of one image: C2R of the size-N spectrum keeping
 // [0, My) x [0, Mx), R2C at size M, scaled by 1/(Mx*My) so that the size-M correlation
 // carries the same Nx*Ny factor as the size-N one.
+static fastfft_status red_prepare_image_on(fastfft_handle h, const void* image_spectrum, int mx, int my);
+
+// Wait on `stream` for a preparation still running on the side stream.
+static fastfft_status join_prep(fastfft_handle h) {
+    if (!h->prep_join_pending) return FASTFFT_OK;
+    h->prep_join_pending = false;
+    const cudaError_t e = cudaStreamWaitEvent(h->stream, h->prep_join, 0);
+    return e == cudaSuccess ? FASTFFT_OK : cuda_fail(h, e, "joining the image preparation");
+}
+
 static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spectrum, int mx, int my) {
     if (h->image_reuse && h->prepared_image == image_spectrum && h->prepared_mx == mx && h->prepared_my == my)
         return FASTFFT_OK;
+    FFB_TRY(join_prep(h));
+    int dev = -1;
+    const bool side = h->prep_stream && cudaGetDevice(&dev) == cudaSuccess && dev == h->prep_device;
+    if (!side) return red_prepare_image_on(h, image_spectrum, mx, my);
+    // fork after everything already on `stream` (earlier fused passes still read region C's
+    // spectrum), prepare on the side stream, record the join for the next column pass
+    cudaError_t e = cudaEventRecord(h->prep_fork, h->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->prep_stream, h->prep_fork, 0);
+    if (e != cudaSuccess) return cuda_fail(h, e, "forking the image preparation");
+    cudaStream_t main_stream = h->stream;
+    h->stream = h->prep_stream;
+    fastfft_status st = red_prepare_image_on(h, image_spectrum, mx, my);
+    h->stream = main_stream;
+    e = cudaEventRecord(h->prep_join, h->prep_stream);
+    if (e != cudaSuccess) {
+        // the side stream's work cannot be joined through the event: wait for it here
+        cudaStreamSynchronize(h->prep_stream);
+        return st != FASTFFT_OK ? st : cuda_fail(h, e, "joining the image preparation");
+    }
+    h->prep_join_pending = true;
+    if (st != FASTFFT_OK) join_prep(h);
+    return st;
+}
+
+static fastfft_status red_prepare_image_on(fastfft_handle h, const void* image_spectrum, int mx, int my) {
     h->prepared_image = nullptr;
     const int nx = (int)h->fwd_out.x, ny = (int)h->fwd_out.y;
     char* c = region_c(h);
@@ -802,6 +870,9 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int mx, int my, int n, c
     }
     if ((e = launch_r2c_rows(mx, h->input_dtype, a, h->stream)) != cudaSuccess) return cuda_fail(h, e, "r2c row pass");
     h->launches++;
+    // the column pass reads the prepared spectrum (the R2C above overlapped its preparation;
+    // the wait falls into the R2C's timing mark)
+    FFB_TRY(join_prep(h));
     prof_mark(h);
     if ((e = twiddles_for(my, &tw)) != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     XcorrColArgs c;

@@ -70,6 +70,16 @@ struct fastfft_plan_s {
     cudaStream_t stream = cudaStreamPerThread;
     std::string last_error;
 
+    // The image preparation of the reduced-size path runs on a second stream of this plan
+    // (higher priority), forked from `stream` after all earlier work and joined back before
+    // the first fused column pass that reads the prepared spectrum, so that it overlaps the
+    // templates' row R2C (which does not read the image).  Null when it could not be created:
+    // the preparation then runs on `stream`.
+    cudaStream_t prep_stream = nullptr;
+    cudaEvent_t prep_fork = nullptr, prep_join = nullptr;
+    int prep_device = -1;
+    bool prep_join_pending = false;  // prep_join recorded and not yet waited on by `stream`
+
     // kernels launched through this handle (fastfft_launch_count)
     long long launches = 0;
 
