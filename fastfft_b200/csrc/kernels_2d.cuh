@@ -147,24 +147,26 @@ r2c_rows_kernel(RowFwdArgs a) {
 #pragma unroll
     for (int q = 0; q < 16; q++) s[phys(j + T * q)] = v[q];
     __syncthreads();
-    const int items = FPB * a.kmax;
+    // item it of this thread: spectrum index k = k0 + T it of FFT ff0
     constexpr int kItemsPerThread = (FPB * (N / 2 + 1) + T * FPB - 1) / (T * FPB);
+    const int ff0 = threadIdx.x % FPB;
+    const int k0 = threadIdx.x / FPB;
+    const float2* sf = smem + ff0 * G::STRIDE;
+    const int rr0 = 2 * (blockIdx.x * FPB + ff0);
+    const bool two = rr0 + 1 < n_rows, one = rr0 < n_rows;
+    float2* o = out_g + (long long)k0 * a.out_pitch + rr0;
+    const long long step = (long long)T * a.out_pitch;
 #pragma unroll
-    for (int it = 0; it < kItemsPerThread; it++) {
-        const int i = threadIdx.x + it * (T * FPB);
-        if (i >= items) continue;
-        const int ff = i % FPB;
-        const int k = i / FPB;
-        const float2* sf = smem + ff * G::STRIDE;
+    for (int it = 0; it < kItemsPerThread; it++, o += step) {
+        const int k = k0 + T * it;
+        if (k >= a.kmax) continue;
         const float2 z1 = sf[phys(k)];
         const float2 z2 = sf[phys((N - k) & (N - 1))];
         const float2 A = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
         const float2 B = make_float2(0.5f * (z1.y + z2.y), 0.5f * (z2.x - z1.x));
-        const int rr = 2 * (blockIdx.x * FPB + ff);
-        float2* o = out_g + (long long)k * a.out_pitch + rr;
-        if (rr + 1 < n_rows) {
+        if (two) {
             *reinterpret_cast<float4*>(o) = make_float4(A.x, A.y, B.x, B.y);
-        } else if (rr < n_rows) {
+        } else if (one) {
             *o = A;
         }
     }
@@ -321,34 +323,36 @@ c2r_rows_kernel(RowInvArgs a) {
     // and k = N/2 bins are dropped, as a C2R of a Hermitian spectrum does.
     // (H + 1) / T <= 9 items per thread: all of a thread's loads are issued before any of
     // them is used, so they are in flight together.
-    const int items = FPB * (H + 1);
+    // Item it of this thread is spectrum index k = k0 + T it of FFT ff0 (the block's item
+    // stride T FPB is a multiple of FPB): one pointer, advanced by T rows per item.
     constexpr int kItemsPerThread = (FPB * (H + 1) + T * FPB - 1) / (T * FPB);
+    const int ff0 = threadIdx.x % FPB;
+    const int k0 = threadIdx.x / FPB;
     float4 ld[kItemsPerThread];
+    {
+        const int rr0 = 2 * (blockIdx.x * FPB + ff0);
+        const bool two = rr0 + 1 < a.n_rows, one = rr0 < a.n_rows;
+        const float2* p = a.in + (long long)blockIdx.y * a.in_batch_stride + (long long)k0 * a.in_pitch + rr0;
+        const long long step = (long long)T * a.in_pitch;
 #pragma unroll
-    for (int it = 0; it < kItemsPerThread; it++) {
-        const int i = threadIdx.x + it * (T * FPB);
-        const int ff = i % FPB;
-        const int k = i / FPB;
-        const int rr = 2 * (blockIdx.x * FPB + ff);
-        const float2* p = a.in + (long long)blockIdx.y * a.in_batch_stride + (long long)k * a.in_pitch + rr;
-        ld[it] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (i < items) {
-            if (rr + 1 < a.n_rows) {
-                ld[it] = *reinterpret_cast<const float4*>(p);
-            } else if (rr < a.n_rows) {
-                const float2 t = *p;
-                ld[it] = make_float4(t.x, t.y, 0.f, 0.f);
+        for (int it = 0; it < kItemsPerThread; it++, p += step) {
+            ld[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k0 + T * it <= H) {
+                if (two) {
+                    ld[it] = *reinterpret_cast<const float4*>(p);
+                } else if (one) {
+                    const float2 t = *p;
+                    ld[it] = make_float4(t.x, t.y, 0.f, 0.f);
+                }
             }
         }
     }
 #pragma unroll
     for (int it = 0; it < kItemsPerThread; it++) {
-        const int i = threadIdx.x + it * (T * FPB);
-        if (i < items) {
-            const int ff = i % FPB;
-            const int k = i / FPB;
+        const int k = k0 + T * it;
+        if (k <= H) {
             const float2 A = make_float2(ld[it].x, ld[it].y), B = make_float2(ld[it].z, ld[it].w);
-            float2* sf = smem + ff * G::STRIDE;
+            float2* sf = smem + ff0 * G::STRIDE;
             if (k == 0 || k == H) {
                 sf[phys(k)] = make_float2(A.x, B.x);
             } else {

@@ -65,24 +65,26 @@ r2c3_rows_kernel(RowFwdArgs a) {
     // Split Z = A + iB into the two real-row spectra (every FFT's buffer is read by the
     // whole block): A[k] = (Z[k] + conj Z[N-k]) / 2, B[k] = -i (Z[k] - conj Z[N-k]) / 2.
     __syncthreads();
-    const int items = FPB * a.kmax;
+    // item it of this thread: spectrum index k = k0 + T it of FFT ff0
     constexpr int kItemsPerThread = (FPB * (N / 2 + 1) + T * FPB - 1) / (T * FPB);
+    const int ff0 = threadIdx.x % FPB;
+    const int k0 = threadIdx.x / FPB;
+    const float2* sf = smem + ff0 * G::STRIDE;
+    const int rr0 = 2 * (blockIdx.x * FPB + ff0);
+    const bool two = rr0 + 1 < n_rows, one = rr0 < n_rows;
+    float2* o = out_g + (long long)k0 * a.out_pitch + rr0;
+    const long long step = (long long)T * a.out_pitch;
 #pragma unroll
-    for (int it = 0; it < kItemsPerThread; it++) {
-        const int i = threadIdx.x + it * (T * FPB);
-        if (i >= items) continue;
-        const int ff = i % FPB;
-        const int k = i / FPB;
-        const float2* sf = smem + ff * G::STRIDE;
+    for (int it = 0; it < kItemsPerThread; it++, o += step) {
+        const int k = k0 + T * it;
+        if (k >= a.kmax) continue;
         const float2 z1 = sf[loc3<P>(k)];
         const float2 z2 = sf[loc3<P>(k == 0 ? 0 : N - k)];
         const float2 A = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
         const float2 B = make_float2(0.5f * (z1.y + z2.y), 0.5f * (z2.x - z1.x));
-        const int rr = 2 * (blockIdx.x * FPB + ff);
-        float2* o = out_g + (long long)k * a.out_pitch + rr;
-        if (rr + 1 < n_rows) {
+        if (two) {
             *reinterpret_cast<float4*>(o) = make_float4(A.x, A.y, B.x, B.y);
-        } else if (rr < n_rows) {
+        } else if (one) {
             *o = A;
         }
     }
@@ -119,30 +121,32 @@ c2r3_rows_kernel(RowInvArgs a) {
     G g(smem, f, k2);
     // Gather rows (2 per FFT) and build Z[k] = A[k] + i B[k] over the full circle from the
     // half spectra; the imaginary parts of the k = 0 and k = N/2 bins are dropped.
-    const int items = FPB * (H + 1);
+    // Item it of this thread is spectrum index k = k0 + T it of FFT ff0 (the block's item
+    // stride T FPB is a multiple of FPB): one pointer, advanced by T rows per item.
     constexpr int kItemsPerThread = (FPB * (H + 1) + T * FPB - 1) / (T * FPB);
+    const int ff0 = threadIdx.x % FPB;
+    const int k0 = threadIdx.x / FPB;
     float4 ld[kItemsPerThread];
+    {
+        const int rr0 = 2 * (blockIdx.x * FPB + ff0);
+        const bool two = rr0 + 1 < a.n_rows, one = rr0 < a.n_rows;
+        const float2* p = a.in + (long long)blockIdx.y * a.in_batch_stride + (long long)k0 * a.in_pitch + rr0;
+        const long long step = (long long)T * a.in_pitch;
 #pragma unroll
-    for (int it = 0; it < kItemsPerThread; it++) {
-        const int i = threadIdx.x + it * (T * FPB);
-        const int ff = i % FPB;
-        const int k = i / FPB;
-        const int rr = 2 * (blockIdx.x * FPB + ff);
-        const float2* p = a.in + (long long)blockIdx.y * a.in_batch_stride + (long long)k * a.in_pitch + rr;
-        ld[it] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (i < items) {
-            if (rr + 1 < a.n_rows) {
-                ld[it] = *reinterpret_cast<const float4*>(p);
-            } else if (rr < a.n_rows) {
-                const float2 x = *p;
-                ld[it] = make_float4(x.x, x.y, 0.f, 0.f);
+        for (int it = 0; it < kItemsPerThread; it++, p += step) {
+            ld[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k0 + T * it <= H) {
+                if (two) {
+                    ld[it] = *reinterpret_cast<const float4*>(p);
+                } else if (one) {
+                    const float2 x = *p;
+                    ld[it] = make_float4(x.x, x.y, 0.f, 0.f);
+                }
             }
         }
     }
-    // Item it of this thread has k = k0 + T it and T = 3 T': k % 3 and (N - k) % 3 stay fixed
-    // and k / 3 moves by T' per item, so the divisions by 3 are done once.
-    const int ff0 = threadIdx.x % FPB;
-    const int k0 = threadIdx.x / FPB;
+    // k % 3 and (N - k) % 3 stay fixed over the items (T = 3 T') and k / 3 moves by T' per
+    // item, so the divisions by 3 are done once.
     float2* const sf = smem + ff0 * G::STRIDE;
     const int kq0 = k0 / 3, kr0 = k0 - 3 * (k0 / 3);
     const int nq0 = (N - k0) / 3, nr0 = (N - k0) - 3 * ((N - k0) / 3);
