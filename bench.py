@@ -336,6 +336,44 @@ def run_low_precision(dev, images_f32, templates_f32, storage, steps, warmup=3):
     return result, check
 
 
+def run_tensor_core(dev, images, templates, steps, warmup=3):
+    """The headline workload (FP32 storage) with the fused column pass's radix-16 passes on
+    the tensor cores in BF16 split precision (SetTensorCoreDFT); same steps as the main leg.
+    Returns the result and template 0's window against image 0 for the accuracy check."""
+    import torch
+
+    import fastfft_b200 as F
+    from fastfft_b200.autotune import tune
+
+    ft = F.FourierTransformer()
+    ft.SetForwardFFTPlan(L, L, 1, N, N, 1)
+    ft.SetInverseFFTPlan(N, N, 1, W, W, 1)
+    ft.SetTensorCoreDFT(True)
+    B = templates.shape[0]
+    outputs = torch.empty(B, ft.ReturnInvOutputMemorySize(), dtype=torch.float32, device=dev)
+    ins = [templates[i] for i in range(B)]
+    outs = [outputs[i] for i in range(B)]
+    per_launch = tune(ft, ins, images[0], outs)
+    for i in range(warmup):
+        ft.FwdImageInvFFTMany(ins, images[i % len(images)], outs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(steps):
+        ft.FwdImageInvFFTMany(ins, images[i % len(images)], outs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ft.FwdImageInvFFTMany(ins[:1], images[0], outs[:1])
+    torch.cuda.synchronize()
+    result = {"value": steps * B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
+              "active": ft.TensorCoreDFTActive(), "correlation_size": list(ft.CorrelationSize()),
+              "templates_per_launch": per_launch,
+              "how": "FP32 storage; the fused column pass's 16-point DFTs as BF16 hi/lo matrix products "
+                     "(mma.sync m16n8k16, FP32 accumulation), everything else FP32"}
+    return result, outputs[0].cpu().numpy()
+
+
 # ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
@@ -623,6 +661,10 @@ def run_ours(args, world, rank, local):
             r, chk = run_low_precision(dev, images, templates, storage, args.steps)
             low.append(r)
             low_checks[storage] = chk
+    tensor_core = None
+    tc_window = None
+    if rank == 0 and not args.skip_uneven:
+        tensor_core, tc_window = run_tensor_core(dev, images, templates, args.steps)
 
     # ---- CPU baseline (rank 0, one GPU) and accuracy check of one window ----
     cpu = None
@@ -663,6 +705,10 @@ def run_ours(args, world, rank, local):
             got_q = O.real_from_padded(chk["window"], (W, W, 1))
             r["accuracy"] = {"rel_l2_vs_fp64_of_stored_inputs": O.rel_l2(got_q, ref_q),
                              "peak_index_equals_fp32_path": bool(O.peak(got_q)[0] == gi)}
+        if tensor_core is not None:
+            got_tc = O.real_from_padded(tc_window, (W, W, 1))
+            tensor_core["accuracy"] = {"rel_l2_vs_fp64": O.rel_l2(got_tc, ref), "rel_max_vs_fp64": O.rel_max(got_tc, ref),
+                                       "peak_index_equals_fp32_path": bool(O.peak(got_tc)[0] == gi)}
 
     if rank == 0:
         line = {
@@ -696,7 +742,8 @@ def run_ours(args, world, rank, local):
             "clocks": clk,
             "cufft_pad_then_transform": cufft,
             "accuracy": accuracy,
-            "uneven_batch": uneven, "low_precision_storage": low, "plain_api": plain,
+            "uneven_batch": uneven, "low_precision_storage": low, "tensor_core_split": tensor_core,
+            "plain_api": plain,
         }
         print(json.dumps(line), flush=True)
 

@@ -669,6 +669,23 @@ fastfft_status fastfft_set_stream(fastfft_handle h, void* cuda_stream) {
     return FASTFFT_OK;
 }
 
+fastfft_status fastfft_set_tensor_core_dft(fastfft_handle h, int enable) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    h->tc_dft = enable != 0;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_tensor_core_dft_active(fastfft_handle h, int* active) {
+    if (!h || !active) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null handle or output pointer");
+    *active = 0;
+    fastfft_status st = validate(h);
+    if (st != FASTFFT_OK) return st;
+    fastfft_plan_s sized = *h;  // the buffer plan of the current settings, without touching h
+    size_buffers(&sized);
+    *active = (h->tc_dft && sized.red_ok && !h->force_full_size && sized.red_my == 3 * 512) ? 1 : 0;
+    return FASTFFT_OK;
+}
+
 fastfft_status fastfft_set_image_reuse(fastfft_handle h, int enable) {
     if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
     h->image_reuse = enable != 0;
@@ -887,6 +904,7 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int mx, int my, int n, c
     c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
     c.intra_scale = intra_op ? intra_op->scale : 1.f;
     c.tw = tw; c.err = h->dev_err;
+    c.tc = h->tc_dft ? 1 : 0;
     if ((e = launch_xcorr_cols(my, FASTFFT_DTYPE_C64, c, h->stream)) != cudaSuccess)
         return cuda_fail(h, e, "cross-correlation column pass");
     h->launches++;

@@ -12,6 +12,7 @@
 #pragma once
 
 #include "fft3.cuh"
+#include "fft_tc.cuh"
 #include "kernels_xcorr.cuh"
 
 namespace ffb {
@@ -336,10 +337,13 @@ struct Xcorr3Smem {
 // instead of 1.58 at 768; a budget of 576 threads (96 registers) spills and loses at 1536.
 constexpr int kXcorr3SmThreads = 384;
 
-template <int P, class ImgC, int FPB, bool MUL>
+// TC: the sub-FFTs' radix-16 passes on the tensor cores in BF16 split precision (fft_tc.cuh;
+// P = 512 only, where a sub-FFT is one warp)
+template <int P, class ImgC, int FPB, bool MUL, bool TC = false>
 __global__ void __launch_bounds__(Fft3Shape<P>::T * FPB,
                                   Fft3Shape<P>::T * FPB < kXcorr3SmThreads ? kXcorr3SmThreads / (Fft3Shape<P>::T * FPB) : 1)
 xcorr3_cols_kernel(XcorrColArgs a) {
+    static_assert(!TC || P == 512, "tensor-core sub-FFTs are one warp (P = 512)");
     using S3 = Fft3Shape<P>;
     using SM = Xcorr3Smem<P, ImgC, FPB>;
     constexpr int T = S3::T;
@@ -374,6 +378,8 @@ xcorr3_cols_kernel(XcorrColArgs a) {
     const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
     const int rounds = (nb + FPB - 1) / FPB;
     Fft3Group<P, FPB, kXcorr3DB> grp(xch, f, k2);
+    TcDft16 tc_f;
+    if constexpr (TC) tc_f.init(j);
 #pragma unroll 1
     for (int it = 0; it < rounds; it++) {
         const int gl = it * FPB + f;                 // template within the block
@@ -408,7 +414,10 @@ xcorr3_cols_kernel(XcorrColArgs a) {
                 v[q] = dif_input<P>(x0, x1, x2, n1, k2, a.tw3);
             }
         }
-        BlockFft<P, false>::run(v, grp, j, a.tw, live ? leading_slots3<P>(Lg, j) : 0);
+        if constexpr (TC)
+            tc_fft512<false>(v, grp.begin(), tc_f, a.tw, j);
+        else
+            BlockFft<P, false>::run(v, grp, j, a.tw, live ? leading_slots3<P>(Lg, j) : 0);
         if constexpr (MUL) {
             // CONJ_MUL (scale 1) skips the 32 multiplies of the scaling
             if (sc == 1.f) {
@@ -422,7 +431,10 @@ xcorr3_cols_kernel(XcorrColArgs a) {
                 }
             }
         }
-        BlockFft<P, true>::run(v, grp, j, a.tw, 16);
+        if constexpr (TC)
+            tc_fft512<true>(v, grp.begin(), tc_f, a.tw, j);
+        else
+            BlockFft<P, true>::run(v, grp, j, a.tw, 16);
         float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
         const int W = live ? a.W : 0;
         dit_output<P>(v, grp, j, t, a.tw3, [&](int n, float2 x) {

@@ -61,6 +61,8 @@ struct XcorrColArgs {
     int L_g[kMaxBatch];        // per-template valid rows of uneven batches (0: use L)
     int tpb;                   // templates per block: block (c, y) serves templates
                                // [y tpb, min((y + 1) tpb, n_batch)) of column c (grid.y blocks)
+    int tc;                    // 1: radix-16 passes on the tensor cores in BF16 split precision
+                               // where the kernel has that form (3P lengths with P = 512)
 };
 
 // Shared-memory plan of the kernel (bytes), shared by the host launcher.

@@ -186,10 +186,12 @@ static cudaError_t xcorr3_impl(const XcorrColArgs& a0, cudaStream_t st) {
     XcorrColArgs a = a0;
     cudaError_t e = tables3(P, &a.tw, &a.tw3);
     if (e != cudaSuccess) return e;
-    static std::atomic<int> set_mul[64], set_nomul[64];
+    static std::atomic<int> set_attr[4][64];
     const bool mul = a.intra_kind != 0;
+    const bool tc = a.tc != 0 && P == 512;
     auto fn = mul ? xcorr3_cols_kernel<P, ImgC, FPB, true> : xcorr3_cols_kernel<P, ImgC, FPB, false>;
-    if ((e = ensure_smem_at_least((const void*)fn, (size_t)smem, mul ? set_mul : set_nomul)) != cudaSuccess) return e;
+    if (tc) fn = mul ? xcorr3_cols_kernel<P, ImgC, FPB, true, P == 512> : xcorr3_cols_kernel<P, ImgC, FPB, false, P == 512>;
+    if ((e = ensure_smem_at_least((const void*)fn, (size_t)smem, set_attr[2 * tc + mul])) != cudaSuccess) return e;
     fn<<<dim3(a.n_cols, (a.n_batch + a.tpb - 1) / a.tpb), Fft3Shape<P>::T * FPB, smem, st>>>(a);
     return cudaGetLastError();
 }

@@ -59,6 +59,7 @@ struct fastfft_plan_s {
     // when the next call names the same address; cleared whenever region C may have been
     // rewritten or the work moved to another stream.
     bool image_reuse = false;
+    bool tc_dft = false;            // fastfft_set_tensor_core_dft
     const void* prepared_image = nullptr;
     long long prepared_mx = 0, prepared_my = 0;   // the size it was prepared at
     int red_batch = 16;             // templates per launch in the reduced-size path

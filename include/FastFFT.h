@@ -144,6 +144,11 @@ class FourierTransformer {
     void SetStream(cudaStream_t stream) { check(fastfft_set_stream(h_, stream), "SetStream"); }
     // Extension: declare that image spectra do not change while in use (fastfft_set_image_reuse).
     void SetImageReuse(bool enable = true) { check(fastfft_set_image_reuse(h_, enable ? 1 : 0), "SetImageReuse"); }
+    // Extension: radix-16 passes of the batched correlation on the tensor cores in BF16 split
+    // precision (fastfft_set_tensor_core_dft).
+    void SetTensorCoreDFT(bool enable = true) {
+        check(fastfft_set_tensor_core_dft(h_, enable ? 1 : 0), "SetTensorCoreDFT");
+    }
 
     template <class PreOpType = std::nullptr_t, class IntraOpType = std::nullptr_t>
     void FwdFFT(InputType* input_ptr, InputType* output_ptr = nullptr, PreOpType pre_op = nullptr,

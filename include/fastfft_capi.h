@@ -184,6 +184,16 @@ FASTFFT_API fastfft_status fastfft_set_full_size_correlation(fastfft_handle h, i
  * which forgets the prepared image).  Changing the plan, the stream or the plan's settings
  * also forgets it.  Default off.  No reference counterpart. */
 FASTFFT_API fastfft_status fastfft_set_image_reuse(fastfft_handle h, int enable);
+/* enable != 0 runs the radix-16 passes of the batched correlation's fused column pass on the
+ * tensor cores in BF16 split precision (hi/lo parts, FP32 accumulation; about 1e-5 relative
+ * L2 against FP64 instead of about 6e-7) where the pass has that form: correlation length
+ * 3 * 512 = 1536 along y.  Every other pass and size keeps the FP32 CUDA-core FFTs.  It is
+ * slower than the FP32 form on B200 (the FFT's butterflies cost less than the split matrix
+ * products).  Default off.  No reference counterpart (the reference computes in FP32). */
+FASTFFT_API fastfft_status fastfft_set_tensor_core_dft(fastfft_handle h, int enable);
+/* *active = 1 when the batched correlation of this plan runs tensor-core passes (the option
+ * is on and the plan correlates at length 1536 along y), else 0. */
+FASTFFT_API fastfft_status fastfft_tensor_core_dft_active(fastfft_handle h, int* active);
 /* Transform size {x, y} that fastfft_fwd_image_inv_many uses for this plan. */
 FASTFFT_API fastfft_status fastfft_correlation_size(fastfft_handle h, int dims[2]);
 

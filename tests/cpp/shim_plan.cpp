@@ -18,6 +18,7 @@ int main(int argc, char**) {
         ft.FwdImageInvFFTMany(0, nullptr, nullptr, nullptr, nullptr, conj_mul, nullptr);
         ft.FwdImageInvFFTManyMip(0, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, conj_mul, nullptr);
         ft.SetImageReuse(true);
+        ft.SetTensorCoreDFT(true);
     }
     FastFFT::FourierTransformer<float, __half, __half2, 3> ft3;
     ft3.SetForwardFFTPlan(64, 64, 64, 256, 256, 256);

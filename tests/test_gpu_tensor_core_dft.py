@@ -1,0 +1,87 @@
+"""Split-precision tensor-core option of the batched correlation (fastfft_set_tensor_core_dft):
+the radix-16 passes of the fused column pass at length 1536 run as BF16 hi/lo matrix products
+with FP32 accumulation.  The bound for this form is 1e-4 relative L2 against FP64, and the
+peak must stay where the FP32 path puts it.
+"""
+import numpy as np
+import pytest
+
+import fastfft_b200 as F
+from oracle import fastfft_oracle as O
+from tests._util import dev, empty, host
+
+pytestmark = pytest.mark.gpu
+
+RTOL_L2_TC = 1e-4
+
+FIN, FOUT, IOUT = (64, 200, 1), (2048, 2048, 1), (200, 1100, 1)    # correlates at (384, 1536)
+
+
+def plan(tc):
+    ft = F.FourierTransformer()
+    ft.SetForwardFFTPlan(*FIN, *FOUT)
+    ft.SetInverseFFTPlan(*FOUT, *IOUT)
+    ft.SetTensorCoreDFT(tc)
+    return ft
+
+
+def test_active_only_where_the_pass_has_that_form(torch_cuda):
+    assert plan(True).TensorCoreDFTActive()
+    assert not plan(False).TensorCoreDFTActive()
+    other = F.FourierTransformer()
+    other.SetForwardFFTPlan(64, 64, 1, 1024, 1024, 1)
+    other.SetInverseFFTPlan(1024, 1024, 1, 256, 256, 1)              # correlates at 384^2
+    other.SetTensorCoreDFT(True)
+    assert not other.TensorCoreDFTActive()
+    forced = plan(True)
+    forced.SetFullSizeCorrelation(True)
+    assert not forced.TensorCoreDFTActive()
+
+
+def test_split_precision_matches_oracle_and_fp32_peaks(torch_cuda):
+    torch = torch_cuda
+    img = O.gaussian_blob_image(2048, n_blobs=8, seed=41)
+    spec = O.image_spectrum_fp32(img)
+    d_spec = dev(torch, spec.view(np.float32))
+    rng = np.random.default_rng(42)
+    # templates cut from the image at lags inside the window, plus noise: a clear peak there
+    ts = []
+    for i in range(5):
+        y0, x0 = rng.integers(0, IOUT[1] - 100), rng.integers(0, IOUT[0] - 20)
+        t = img[y0:y0 + FIN[1], x0:x0 + FIN[0]].astype(np.float32) + 0.1 * rng.standard_normal((FIN[1], FIN[0]))
+        ts.append(t.astype(np.float32))
+    d_ts = [dev(torch, O.real_to_padded(t, FIN)) for t in ts]
+    tc, fp = plan(True), plan(False)
+    out_tc = [empty(torch, tc.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    out_fp = [empty(torch, fp.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    tc.FwdImageInvFFTMany(d_ts, d_spec, out_tc)
+    fp.FwdImageInvFFTMany(d_ts, d_spec, out_fp)
+    torch.cuda.synchronize()
+    p = O.Plan(FIN, FOUT, FOUT, IOUT)
+    for t, a, b in zip(ts, out_tc, out_fp):
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, FIN), spec, p, out_dtype=np.float64), IOUT)
+        got_tc = O.real_from_padded(host(a), IOUT)
+        got_fp = O.real_from_padded(host(b), IOUT)
+        err_tc = O.rel_l2(got_tc, ref)
+        assert err_tc <= RTOL_L2_TC
+        assert err_tc > O.rel_l2(got_fp, ref)            # the split form is the less accurate one
+        assert O.peak(got_tc)[0] == O.peak(got_fp)[0] == O.peak(ref)[0]
+
+
+def test_low_precision_image_with_tensor_core_passes(torch_cuda):
+    torch = torch_cuda
+    spec = O.image_spectrum_fp32(O.gaussian_blob_image(2048, n_blobs=4, seed=43)) / 2048
+    ft = F.FourierTransformer(image_dtype="complex_bf16")
+    ft.SetForwardFFTPlan(*FIN, *FOUT)
+    ft.SetInverseFFTPlan(*FOUT, *IOUT)
+    ft.SetTensorCoreDFT(True)
+    assert ft.TensorCoreDFTActive()
+    spec_bf = torch.from_numpy(spec.view(np.float32).copy()).to(torch.bfloat16).cuda()
+    spec_deq = spec_bf.float().cpu().numpy().view(np.complex64).reshape(spec.shape)
+    t = np.random.default_rng(44).standard_normal((FIN[1], FIN[0])).astype(np.float32)
+    out = empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32)
+    ft.FwdImageInvFFTMany([dev(torch, O.real_to_padded(t, FIN))], spec_bf, [out])
+    torch.cuda.synchronize()
+    p = O.Plan(FIN, FOUT, FOUT, IOUT)
+    ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, FIN), spec_deq, p, out_dtype=np.float64), IOUT)
+    assert O.rel_l2(O.real_from_padded(host(out), IOUT), ref) <= RTOL_L2_TC
