@@ -129,6 +129,10 @@ struct Fft3Group {
 
     __device__ __forceinline__ float2* begin_full() { return next_buffer(false); }
     __device__ __forceinline__ float2* begin() { return next_buffer(true) + r * SUB; }
+    // Whole buffer for a step in which each sub-FFT first writes only its own region: the
+    // region's earlier readers in the FFT are that sub-FFT's own threads, so the sub-level
+    // wait suffices (the caller's reads across regions follow a sync_fft()).
+    __device__ __forceinline__ float2* begin_own() { return next_buffer(true); }
 };
 
 constexpr float kH3 = 0.866025403784438646764f;  // sqrt(3)/2
@@ -162,13 +166,15 @@ __device__ __forceinline__ float2 dif_input(float2 x0, float2 x1, float2 x2, int
 }
 
 // Final radix-3 pass of the inverse.  v: z_k2[n1] of thread (k2 = g.r, j), n1 = j + T' q.
-// Writes them to the next buffer, waits for the FFT's threads, then thread t produces
-// x[n1], x[n1 + P], x[n1 + 2P] for n1 = t + T i and hands each to store(n, value).
+// Writes them to region k2 of the next buffer, waits for the FFT's threads, then thread t
+// produces x[n1], x[n1 + P], x[n1 + 2P] for n1 = t + T i and hands each to store(n, value).
+// The cross-region reads here must be followed by a sync_fft() before any later write to the
+// buffer (the batched kernel's next template begins with one).
 template <int P, class G, class Store>
 __device__ __forceinline__ void dit_output(float2 (&v)[16], G& g, int j, int t, const float2* __restrict__ tw3,
                                            Store store) {
     using S3 = Fft3Shape<P>;
-    float2* buf = g.begin_full();
+    float2* buf = g.begin_own();
     {
         float2* s = buf + g.r * G::SUB;
 #pragma unroll
@@ -203,7 +209,7 @@ __device__ __forceinline__ float2* forward_dit(float2 (&v)[16], G& g, int j, int
                                                const float2* __restrict__ tw3, int qnz) {
     using S3 = Fft3Shape<P>;
     BlockFft<P, false>::run(v, g, j, tw, qnz);
-    float2* buf = g.begin_full();
+    float2* buf = g.begin_own();
     {
         float2* s = buf + g.r * G::SUB;
 #pragma unroll
