@@ -401,13 +401,15 @@ ColArgs col_args(const void* in, long long in_stride, int L, void* out, long lon
 
 enum StageMode { ST_FWD, ST_INV, ST_XCORR };
 
+// dtype: the spectrum's storage for ST_FWD (written), the input's for ST_INV, the image's for
+// ST_XCORR
 fastfft_status stage_cols(fastfft_plan_s* h, int n, StageMode mode, int dtype, ColArgs& c) {
     const float2* tw = nullptr;
     cudaError_t e = twiddles_for(n, &tw);
     if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     c.tw = tw;
     if (mode == ST_FWD)
-        e = launch_cols_fwd(n, c, h->stream);
+        e = launch_cols_fwd(n, dtype, c, h->stream);
     else if (mode == ST_INV)
         e = launch_cols_inv(n, dtype, c, h->stream);
     else
@@ -435,7 +437,8 @@ fastfft_status seq_fwd(fastfft_plan_s* h, const void* in, void* out, float pre_s
         FFB_TRY(stage_r2c(h, nx, h->input_dtype, in, 2LL * fi.w, (int)fi.y, (int)fi.y, 1, (int)fi.x, region_a(h),
                           h->pitch_a, kmax, pre_scale));
         ColArgs c = col_args(region_a(h), h->pitch_a, (int)fi.y, out, fo.y, (int)fo.y, kmax);
-        return stage_cols(h, ny, ST_FWD, FASTFFT_DTYPE_C64, c);
+        c.out_scale = h->spec_scale;
+        return stage_cols(h, ny, ST_FWD, h->spec_dtype, c);
     }
     const long long ly = fi.y, lz = fi.z;
     // x: rows (y, z) -> A[kx][y][z]
@@ -449,7 +452,8 @@ fastfft_status seq_fwd(fastfft_plan_s* h, const void* in, void* out, float pre_s
     FFB_TRY(stage_cols(h, nz, ST_FWD, FASTFFT_DTYPE_C64, cz));
     // y: columns (kz, kx) -> spectrum [kz][kx][ky]
     ColArgs cy = col_args(region_b(h), ly, (int)ly, out, fo.y, (int)fo.y, (int)(fo.z * kmax));
-    return stage_cols(h, ny, ST_FWD, FASTFFT_DTYPE_C64, cy);
+    cy.out_scale = h->spec_scale;
+    return stage_cols(h, ny, ST_FWD, h->spec_dtype, cy);
 }
 
 // Inverse from a complex spectrum `in` (dtype in_dtype) of the inverse-input size.
@@ -666,6 +670,17 @@ fastfft_status fastfft_set_stream(fastfft_handle h, void* cuda_stream) {
     cudaStream_t s = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : cudaStreamPerThread;
     if (s != h->stream) h->prepared_image = nullptr;  // a preparation may still run on the old stream
     h->stream = s;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_set_spectrum_output(fastfft_handle h, int dtype, float scale) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (dtype != FASTFFT_DTYPE_C64 && dtype != FASTFFT_DTYPE_C32H && dtype != FASTFFT_DTYPE_C32BF)
+        return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "spectrum storage must be a complex dtype");
+    if (!(scale == scale) || scale == 0.f || scale > 3.0e38f || scale < -3.0e38f)
+        return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "spectrum scale must be finite and non-zero");
+    h->spec_dtype = dtype;
+    h->spec_scale = scale;
     return FASTFFT_OK;
 }
 

@@ -49,6 +49,14 @@ template <> __device__ __forceinline__ float2 ld_cplx<__nv_bfloat162>(const __nv
     return __bfloat1622float2(*p);
 }
 
+// Complex stores (the forward spectrum may be written in FP16 / BF16, rounded to nearest)
+template <class T> __device__ __forceinline__ void st_cplx(T* p, float2 v);
+template <> __device__ __forceinline__ void st_cplx<float2>(float2* p, float2 v) { *p = v; }
+template <> __device__ __forceinline__ void st_cplx<__half2>(__half2* p, float2 v) { *p = __float22half2_rn(v); }
+template <> __device__ __forceinline__ void st_cplx<__nv_bfloat162>(__nv_bfloat162* p, float2 v) {
+    *p = __float22bfloat162_rn(v);
+}
+
 template <class T> __device__ __forceinline__ float2 ld_cplx_stream(const T* p);
 template <> __device__ __forceinline__ float2 ld_cplx_stream<float2>(const float2* p) { return __ldcs(p); }
 template <> __device__ __forceinline__ float2 ld_cplx_stream<__half2>(const __half2* p) {
@@ -262,8 +270,8 @@ cols_kernel(ColArgs a) {
         for (int q = 0; q < 16; q++) {
             const int n = j + T * q - a.W0;
             if (n >= 0 && n < a.W) {
-                float2 x = (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q];
-                pout[n * es] = x;
+                const float2 x = (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q];
+                st_cplx<OutC>(pout + n * es, x);
             }
         }
     }

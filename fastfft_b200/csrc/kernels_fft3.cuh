@@ -235,7 +235,8 @@ c2r3_rows_kernel(RowInvArgs a) {
 // single-template XCORR.  Output window [W0, W0 + W); the general 3D addressing of
 // cols_kernel is not supported at these lengths (3D transforms are powers of two).
 // ---------------------------------------------------------------------------
-template <int P, int MODE, class InC, class ImgC, int FPB>
+// OutC: storage type of the forward spectrum (FWD mode; the other modes write float2)
+template <int P, int MODE, class InC, class ImgC, int FPB, class OutC = float2>
 __global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, (Fft3Shape<P>::T * FPB <= 256) ? 2 : 1)
 cols3_kernel(ColArgs a) {
     using S3 = Fft3Shape<P>;
@@ -277,10 +278,11 @@ cols3_kernel(ColArgs a) {
         if constexpr (MODE == COL_FWD) {
             // spectrum side: X[3 m + k2] straight from the registers
             if (valid) {
+                OutC* po = static_cast<OutC*>(a.out) + bz * a.out_batch_stride + (long long)col * a.out_stride;
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
                     const int n = 3 * (j + TP * q) + k2 - a.W0;
-                    if (n >= 0 && n < a.W) pout[n] = (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q];
+                    if (n >= 0 && n < a.W) st_cplx<OutC>(po + n, (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q]);
                 }
             }
             return;

@@ -18,7 +18,8 @@ struct XcorrColArgs;
 // dtype codes follow fastfft_dtype in include/fastfft_capi.h
 cudaError_t launch_r2c_rows(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
 cudaError_t launch_c2r_rows(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
-cudaError_t launch_cols_fwd(int n, const ColArgs& a, cudaStream_t st);
+// out_dtype: storage of the spectrum written (3 complex64, 4 complex32, 5 complex bf16)
+cudaError_t launch_cols_fwd(int n, int out_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st);
 // Batched fused column pass (TMA-staged image and template columns), n <= 4096.
@@ -29,7 +30,7 @@ size_t xcorr_cols_smem(int n, int img_dtype, int L, int n_batch);
 // 2D plans at these sizes; the public launchers above forward them here.
 cudaError_t launch_r2c3(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
 cudaError_t launch_c2r3(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
-cudaError_t launch_cols3_fwd(int n, const ColArgs& a, cudaStream_t st);
+cudaError_t launch_cols3_fwd(int n, int out_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols3_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols3_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_xcorr3(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st);

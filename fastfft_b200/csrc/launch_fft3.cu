@@ -120,7 +120,7 @@ cudaError_t launch_c2r3(int n, int out_dtype, const RowInvArgs& a, cudaStream_t 
 }
 
 // ---------------------------------------------------------------------------
-template <int P, int MODE, class InC, class ImgC>
+template <int P, int MODE, class InC, class ImgC, class OutC = float2>
 static cudaError_t cols3_impl(const ColArgs& a0, cudaStream_t st) {
     // 2D layout only (3D transforms are powers of two)
     if (a0.in_div > 1 || a0.out_div > 1 || a0.out_elem_stride > 1) return cudaErrorInvalidValue;
@@ -131,7 +131,7 @@ static cudaError_t cols3_impl(const ColArgs& a0, cudaStream_t st) {
     cudaError_t e = tables3(P, &a.tw, &a.tw3);
     if (e != cudaSuccess) return e;
     static std::atomic<unsigned long long> mask{0};
-    auto fn = cols3_kernel<P, MODE, InC, ImgC, FPB>;
+    auto fn = cols3_kernel<P, MODE, InC, ImgC, FPB, OutC>;
     if ((e = ensure_smem_attr((const void*)fn, smem, &mask)) != cudaSuccess) return e;
     const int grid = (a.n_cols + FPB - 1) / FPB;
     if (grid == 0) return cudaSuccess;
@@ -141,8 +141,13 @@ static cudaError_t cols3_impl(const ColArgs& a0, cudaStream_t st) {
 }
 
 template <int P>
-static cudaError_t cols3_fwd_dispatch(const ColArgs& a, cudaStream_t st) {
-    return cols3_impl<P, COL_FWD, float2, float2>(a, st);
+static cudaError_t cols3_fwd_dispatch(int out_dtype, const ColArgs& a, cudaStream_t st) {
+    switch (out_dtype) {
+        case 3: return cols3_impl<P, COL_FWD, float2, float2, float2>(a, st);
+        case 4: return cols3_impl<P, COL_FWD, float2, float2, __half2>(a, st);
+        case 5: return cols3_impl<P, COL_FWD, float2, float2, __nv_bfloat162>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 template <int P>
 static cudaError_t cols3_inv_dispatch(int in_dtype, const ColArgs& a, cudaStream_t st) {
@@ -163,7 +168,9 @@ static cudaError_t cols3_xcorr_dispatch(int img_dtype, const ColArgs& a, cudaStr
     }
 }
 
-cudaError_t launch_cols3_fwd(int n, const ColArgs& a, cudaStream_t st) { FFB_SIZE3_SWITCH(n, cols3_fwd_dispatch, a, st) }
+cudaError_t launch_cols3_fwd(int n, int out_dtype, const ColArgs& a, cudaStream_t st) {
+    FFB_SIZE3_SWITCH(n, cols3_fwd_dispatch, out_dtype, a, st)
+}
 cudaError_t launch_cols3_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st) {
     FFB_SIZE3_SWITCH(n, cols3_inv_dispatch, in_dtype, a, st)
 }

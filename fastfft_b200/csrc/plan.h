@@ -60,6 +60,8 @@ struct fastfft_plan_s {
     // rewritten or the work moved to another stream.
     bool image_reuse = false;
     bool tc_dft = false;            // fastfft_set_tensor_core_dft
+    int spec_dtype = 3;             // fastfft_set_spectrum_output: FwdFFT's spectrum storage
+    float spec_scale = 1.f;         //   and scale
     const void* prepared_image = nullptr;
     long long prepared_mx = 0, prepared_my = 0;   // the size it was prepared at
     int red_batch = 16;             // templates per launch in the reduced-size path

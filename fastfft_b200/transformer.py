@@ -252,6 +252,12 @@ class FourierTransformer:
         changing the plan or stream, forgets the prepared image."""
         self._check(self._lib.fastfft_set_image_reuse(self._h, int(bool(enable))))
 
+    def SetSpectrumOutput(self, dtype="complex64", scale=1.0):
+        """FwdFFT writes its spectrum as `dtype` ("complex64", "complex32" or "complex_bf16"),
+        every value multiplied by `scale` and rounded once: the normalised, quantised image
+        spectrum for FwdImageInvFFT with a matching image_dtype."""
+        self._check(self._lib.fastfft_set_spectrum_output(self._h, _dtype_code(dtype, _CPLX_DTYPES), float(scale)))
+
     def SetTensorCoreDFT(self, enable=True):
         """Run the radix-16 passes of the batched correlation's fused column pass on the tensor
         cores in BF16 split precision (about 1e-5 relative L2 against FP64) where the pass has

@@ -144,6 +144,11 @@ class FourierTransformer {
     void SetStream(cudaStream_t stream) { check(fastfft_set_stream(h_, stream), "SetStream"); }
     // Extension: declare that image spectra do not change while in use (fastfft_set_image_reuse).
     void SetImageReuse(bool enable = true) { check(fastfft_set_image_reuse(h_, enable ? 1 : 0), "SetImageReuse"); }
+    // Extension: FwdFFT writes its spectrum as `dtype` (FASTFFT_DTYPE_C64 / C32H / C32BF), each
+    // value times `scale` (fastfft_set_spectrum_output).
+    void SetSpectrumOutput(int dtype, float scale = 1.f) {
+        check(fastfft_set_spectrum_output(h_, dtype, scale), "SetSpectrumOutput");
+    }
     // Extension: radix-16 passes of the batched correlation on the tensor cores in BF16 split
     // precision (fastfft_set_tensor_core_dft).
     void SetTensorCoreDFT(bool enable = true) {

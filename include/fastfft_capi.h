@@ -97,6 +97,13 @@ FASTFFT_API fastfft_status fastfft_set_stream(fastfft_handle h, void* cuda_strea
 FASTFFT_API fastfft_status fastfft_set_inverse_output_origin(fastfft_handle h, size_t ox, size_t oy, size_t oz);
 /* Real output dtype of InvFFT / FwdImageInvFFT (default: input_dtype, as in the reference). */
 FASTFFT_API fastfft_status fastfft_set_output_dtype(fastfft_handle h, int dtype);
+/* Storage of the spectrum FwdFFT writes: FASTFFT_DTYPE_C64 (default), C32H or C32BF, each
+ * value multiplied by `scale` (1 = as computed) and rounded to nearest once in the last pass:
+ * the normalised, quantised image spectrum that FwdImageInvFFT reads with a matching
+ * image_dtype, written without a separate conversion pass (e.g. scale 1/N against FP16
+ * overflow).  The output buffer then holds ReturnFwdOutputMemorySize() / 2 complex values of
+ * that type.  No reference counterpart (the reference's spectra are FP32). */
+FASTFFT_API fastfft_status fastfft_set_spectrum_output(fastfft_handle h, int dtype, float scale);
 
 /* FwdFFT(input, output, pre_op, intra_op) (FastFFT.h:165-170, FastFFT.cu:263-277).
  * Ops may be NULL (NOOP).  Output: complex64 spectrum [kz][kx][ky]. */

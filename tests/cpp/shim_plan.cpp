@@ -19,6 +19,7 @@ int main(int argc, char**) {
         ft.FwdImageInvFFTManyMip(0, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, conj_mul, nullptr);
         ft.SetImageReuse(true);
         ft.SetTensorCoreDFT(true);
+        ft.SetSpectrumOutput(FASTFFT_DTYPE_C32BF, 1.f / 4096);
     }
     FastFFT::FourierTransformer<float, __half, __half2, 3> ft3;
     ft3.SetForwardFFTPlan(64, 64, 64, 256, 256, 256);

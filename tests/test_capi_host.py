@@ -129,3 +129,15 @@ def test_null_handle_calls_fail_cleanly():
     assert lib.fastfft_wait(None) == C.ERR_INVALID_ARGUMENT
     assert lib.fastfft_destroy(None) == C.OK
     assert lib.fastfft_last_error(None) != b""
+
+
+def test_spectrum_output_setting_is_validated():
+    ft = new()
+    ft.SetSpectrumOutput("complex32", 1.0 / 4096)
+    ft.SetSpectrumOutput("complex_bf16", 0.5)
+    ft.SetSpectrumOutput("complex64")
+    lib = C.lib()
+    assert lib.fastfft_set_spectrum_output(ft._h, C.DTYPE_F32, 1.0) == C.ERR_INVALID_ARGUMENT   # real
+    assert lib.fastfft_set_spectrum_output(ft._h, C.DTYPE_C32H, 0.0) == C.ERR_INVALID_ARGUMENT   # zero
+    assert lib.fastfft_set_spectrum_output(ft._h, C.DTYPE_C32H, float("nan")) == C.ERR_INVALID_ARGUMENT
+    assert lib.fastfft_set_spectrum_output(None, C.DTYPE_C64, 1.0) == C.ERR_INVALID_ARGUMENT
