@@ -1240,6 +1240,12 @@ fastfft_status fastfft_wait(fastfft_handle h) {
     if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamSynchronize");
+    if (h->prep_join_pending) {
+        // an image preparation whose column pass never ran (a failed call): wait for it too
+        h->prep_join_pending = false;
+        e = cudaStreamSynchronize(h->prep_stream);
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamSynchronize (image preparation)");
+    }
     if (h->dev_err) {
         int flag = 0;
         e = cudaMemcpy(&flag, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost);
