@@ -36,8 +36,13 @@ using namespace ffb;
 #define FFB_XCORR_TPB 8
 #endif
 
-// templates that one block of the fused column pass stages for a launch of n
-static inline int xcorr_tpb(int n) { return FFB_XCORR_TPB > 0 && n > FFB_XCORR_TPB ? FFB_XCORR_TPB : n; }
+// templates that one block of the fused column pass stages for a launch of n at column
+// length my; at 1536 (= 3 * 512) six per block measured best on B200 (5.37 instead of 5.47
+// us per template for that pass with 64 per launch; 4, 5 and 8 were slower)
+static inline int xcorr_tpb(int n, long long my) {
+    const int per_block = (FFB_XCORR_TPB == 8 && my == 3 * 512) ? 6 : FFB_XCORR_TPB;
+    return per_block > 0 && n > per_block ? per_block : n;
+}
 
 // Uneven batches: each template correlates at its own exact size class (1), or every
 // template at the plan's size (0).
@@ -210,7 +215,7 @@ void size_buffers(fastfft_plan_s* h) {
             // templates per launch: bounded by the shared memory of the fused column kernel
             h->red_batch = h->red_batch_request;
             while (h->red_batch > 1 &&
-                   xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, xcorr_tpb(h->red_batch)) >
+                   xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, xcorr_tpb(h->red_batch, my)) >
                        226 * 1024)
                 h->red_batch--;
             if (xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, 1) > 226 * 1024) {
@@ -913,7 +918,7 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int mx, int my, int n, c
     c.img = spec; c.img_stride = my;
     c.out = t2; c.out_pitch = h->pitch_b; c.out_batch = h->red_t2_stride; c.W = (int)h->inv_out.y;
     c.n_cols = mx / 2 + 1; c.n_batch = n;
-    c.tpb = xcorr_tpb(n);
+    c.tpb = xcorr_tpb(n, my);
     if (dims)
         for (int g = 0; g < n; g++) c.L_g[g] = dims[2 * g + 1];
     c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
