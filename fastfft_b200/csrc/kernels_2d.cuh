@@ -81,7 +81,8 @@ __device__ __forceinline__ int leading_slots(int L, int j) {
 // ---------------------------------------------------------------------------
 // Row R2C (forward), two rows per complex FFT
 // ---------------------------------------------------------------------------
-// Templates per launch: blockIdx.y selects the template of a batch.
+// Templates per launch: blockIdx.y selects the template of a batch (the row passes take them
+// in reverse order, so that each pass starts on the data its predecessor wrote last).
 // Templates per launch of the batched passes (grid.y).  Up to 64: more templates per launch
 // mean more blocks per launch and a shorter partly empty last wave in all three passes
 // (measured on B200 at 1536^2: 13.8, 12.1 and 11.5 us per template at 16, 32 and 64).
@@ -126,7 +127,9 @@ r2c_rows_kernel(RowFwdArgs a) {
     const int j = threadIdx.x - f * T;
     G g(smem, f);
     float2* s = g.base;
-    const int gb = blockIdx.y;
+    // batch entries in reverse order: the batched column pass that follows starts with entry 0,
+    // whose rows are then the last written and still in L2
+    const int gb = gridDim.y - 1 - blockIdx.y;
     const int n_rows = a.rows_g[gb] > 0 ? a.rows_g[gb] : a.n_rows;
     const int L = a.L_g[gb] > 0 ? a.L_g[gb] : a.L;
     const long long in_pitch = a.pitch_g[gb] > 0 ? a.pitch_g[gb] : a.in_pitch;
@@ -135,7 +138,7 @@ r2c_rows_kernel(RowFwdArgs a) {
     const InT* in_g = static_cast<const InT*>(a.in[gb]);
     const InT* pa = in_g + input_row(ra, a.rows_y, a.rows_z) * in_pitch;
     const InT* pb = in_g + input_row(ra + 1, a.rows_y, a.rows_z) * in_pitch;
-    float2* const out_g = a.out + (long long)blockIdx.y * a.out_batch_stride;
+    float2* const out_g = a.out + (long long)gb * a.out_batch_stride;
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
@@ -326,6 +329,9 @@ c2r_rows_kernel(RowInvArgs a) {
     const int j = threadIdx.x - f * T;
     G g(smem, f);
     float2* s = g.base;
+    // batch entries in reverse order: the batched column pass wrote the last entries last, so
+    // theirs are the columns still in L2
+    const int gb = gridDim.y - 1 - blockIdx.y;
     // Gather rows (2 per FFT) and build Z[k] = A[k] + i B[k] over the full circle
     // from the half spectrum (A, B Hermitian).  The imaginary parts of the k = 0
     // and k = N/2 bins are dropped, as a C2R of a Hermitian spectrum does.
@@ -340,7 +346,7 @@ c2r_rows_kernel(RowInvArgs a) {
     {
         const int rr0 = 2 * (blockIdx.x * FPB + ff0);
         const bool two = rr0 + 1 < a.n_rows, one = rr0 < a.n_rows;
-        const float2* p = a.in + (long long)blockIdx.y * a.in_batch_stride + (long long)k0 * a.in_pitch + rr0;
+        const float2* p = a.in + (long long)gb * a.in_batch_stride + (long long)k0 * a.in_pitch + rr0;
         const long long step = (long long)T * a.in_pitch;
 #pragma unroll
         for (int it = 0; it < kItemsPerThread; it++, p += step) {
@@ -375,7 +381,7 @@ c2r_rows_kernel(RowInvArgs a) {
     for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
     BlockFft<N, true>::run(v, g, j, a.tw, 16);
     const int ra = 2 * (blockIdx.x * FPB + f);
-    OutT* oa = static_cast<OutT*>(a.out[blockIdx.y]) + (long long)ra * a.out_pitch;
+    OutT* oa = static_cast<OutT*>(a.out[gb]) + (long long)ra * a.out_pitch;
     OutT* ob = oa + a.out_pitch;
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
     if (!a.peaks_only) {
@@ -389,7 +395,7 @@ c2r_rows_kernel(RowInvArgs a) {
         }
     }
     if (a.mip) {
-        const unsigned int tmpl = (unsigned)(a.mip_base + a.peak_slot[blockIdx.y]);
+        const unsigned int tmpl = (unsigned)(a.mip_base + a.peak_slot[gb]);
         unsigned long long* ma = a.mip + (long long)ra * a.W;
 #pragma unroll
         for (int q = 0; q < 16; q++) {
@@ -421,7 +427,7 @@ c2r_rows_kernel(RowInvArgs a) {
             const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
             best = other > best ? other : best;
         }
-        if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(a.peaks + a.peak_slot[blockIdx.y], best);
+        if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(a.peaks + a.peak_slot[gb], best);
     }
 }
 
