@@ -69,6 +69,9 @@ SIGNATURES = {
     "fastfft_set_image_reuse": (_st, [Handle, ctypes.c_int]),
     "fastfft_set_tensor_core_dft": (_st, [Handle, ctypes.c_int]),
     "fastfft_set_spectrum_output": (_st, [Handle, ctypes.c_int, ctypes.c_float]),
+    "fastfft_radial_power": (_st, [Handle, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
+    "fastfft_apply_radial_filter": (_st, [Handle, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_int]),
     "fastfft_tensor_core_dft_active": (_st, [Handle, ctypes.POINTER(ctypes.c_int)]),
     "fastfft_fwd_image_inv_many_peaks": (_st, [Handle, ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int),
                                                ctypes.POINTER(_vp), ctypes.POINTER(_vp), _vp, _op, _op, _op]),

@@ -22,6 +22,7 @@
 #include "fft3.cuh"
 #include "kernels_xcorr.cuh"
 #include "launch.h"
+#include "spectrum_ops.h"
 #include "plan.h"
 
 using namespace ffb;
@@ -600,6 +601,10 @@ fastfft_status fastfft_create(fastfft_handle* out, int compute_dtype, int input_
 
 fastfft_status fastfft_destroy(fastfft_handle h) {
     if (!h) return FASTFFT_OK;
+    if (h->radial_scratch) {
+        cudaStreamSynchronize(h->stream);
+        cudaFree(h->radial_scratch);
+    }
     if (h->prep_stream) {
         cudaStreamSynchronize(h->prep_stream);
         cudaEventDestroy(h->prep_fork);
@@ -686,6 +691,63 @@ fastfft_status fastfft_set_spectrum_output(fastfft_handle h, int dtype, float sc
         return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "spectrum scale must be finite and non-zero");
     h->spec_dtype = dtype;
     h->spec_scale = scale;
+    return FASTFFT_OK;
+}
+
+static fastfft_status radial_checks(fastfft_handle h, const void* a, const void* b, int n, int n_bins) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (!a || !b) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null spectrum, filter or output pointer");
+    if (n < 2 || n > 8192 || (n & 1)) return fail(h, FASTFFT_ERR_INVALID_DIMS, "n must be even and in [2, 8192]");
+    if (n_bins < 1 || n_bins > 8192) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "n_bins must be in [1, 8192]");
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_radial_power(fastfft_handle h, const void* spectrum, int n, float* power, int n_bins) {
+    FFB_TRY(radial_checks(h, spectrum, power, n, n_bins));
+    if (h->radial_scratch_bins < n_bins) {
+        if (h->radial_scratch) {
+            cudaStreamSynchronize(h->stream);
+            cudaFree(h->radial_scratch);
+            h->radial_scratch = nullptr;
+            h->radial_scratch_bins = 0;
+        }
+        cudaError_t e = cudaMalloc(&h->radial_scratch, (size_t)2 * n_bins * sizeof(double));
+        if (e != cudaSuccess) {
+            h->radial_scratch = nullptr;
+            return fail(h, FASTFFT_ERR_ALLOC, std::string("cudaMalloc of the radial work array: ") + cudaGetErrorString(e));
+        }
+        h->radial_scratch_bins = n_bins;
+    }
+    RadialArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.in = static_cast<const float2*>(spectrum);
+    a.n = n;
+    a.n_bins = n_bins;
+    a.sums = h->radial_scratch;
+    a.weights = h->radial_scratch + n_bins;
+    const cudaError_t e = launch_radial_power(a, power, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "radial power");
+    h->launches += 2;
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_apply_radial_filter(fastfft_handle h, const void* in, void* out, int n, const float* filter,
+                                           int n_bins) {
+    FFB_TRY(radial_checks(h, in, filter, n, n_bins));
+    if (!out) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null output pointer");
+    if (out == in && h->spec_dtype != FASTFFT_DTYPE_C64)
+        return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "in-place filtering needs complex64 storage");
+    RadialArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.in = static_cast<const float2*>(in);
+    a.out = out;
+    a.n = n;
+    a.n_bins = n_bins;
+    a.filter = filter;
+    a.scale = h->spec_scale;
+    const cudaError_t e = launch_radial_filter(h->spec_dtype, a, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "radial filter");
+    h->launches++;
     return FASTFFT_OK;
 }
 

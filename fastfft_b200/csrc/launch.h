@@ -36,6 +36,11 @@ cudaError_t launch_cols3_xcorr(int n, int img_dtype, const ColArgs& a, cudaStrea
 cudaError_t launch_xcorr3(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st);
 size_t xcorr3_smem(int n, int img_dtype, int L, int n_batch);
 
+// Radial operations on square 2D half spectra (spectrum_ops.cu).
+struct RadialArgs;
+cudaError_t launch_radial_filter(int out_dtype, const RadialArgs& a, cudaStream_t st);
+cudaError_t launch_radial_power(const RadialArgs& a, float* power, cudaStream_t st);
+
 // Device-wide FP64-generated twiddle tables (generated once per device): for a power of
 // two n the radix-16 pass table, for n = 3P the radix-3 pass table W_n^m, m < 2P.
 cudaError_t twiddles_for(int n, const float2** out);

@@ -60,6 +60,8 @@ struct fastfft_plan_s {
     // rewritten or the work moved to another stream.
     bool image_reuse = false;
     bool tc_dft = false;            // fastfft_set_tensor_core_dft
+    double* radial_scratch = nullptr;  // fastfft_radial_power's sums (2 x radial_scratch_bins)
+    int radial_scratch_bins = 0;
     int spec_dtype = 3;             // fastfft_set_spectrum_output: FwdFFT's spectrum storage
     float spec_scale = 1.f;         //   and scale
     const void* prepared_image = nullptr;

@@ -258,6 +258,20 @@ class FourierTransformer:
         spectrum for FwdImageInvFFT with a matching image_dtype."""
         self._check(self._lib.fastfft_set_spectrum_output(self._h, _dtype_code(dtype, _CPLX_DTYPES), float(scale)))
 
+    def RadialPower(self, spectrum, n, power):
+        """power[r] (float32 device tensor of n_bins) = mean |S|^2 over the elements of the n x n
+        complex64 half spectrum `spectrum` at radius r = floor(sqrt(kx^2 + ky^2)); the last bin
+        also holds every larger radius."""
+        self._bind_stream()
+        self._check(self._lib.fastfft_radial_power(self._h, _ptr(spectrum), int(n), _ptr(power), int(power.numel())))
+
+    def ApplyRadialFilter(self, spectrum, output, n, filt):
+        """output = spectrum x filt[r] (radius as in RadialPower), written in the storage and
+        scale set by SetSpectrumOutput; in place only with complex64 storage."""
+        self._bind_stream()
+        self._check(self._lib.fastfft_apply_radial_filter(self._h, _ptr(spectrum), _ptr(output), int(n), _ptr(filt),
+                                                          int(filt.numel())))
+
     def SetTensorCoreDFT(self, enable=True):
         """Run the radix-16 passes of the batched correlation's fused column pass on the tensor
         cores in BF16 split precision (about 1e-5 relative L2 against FP64) where the pass has

@@ -104,6 +104,21 @@ FASTFFT_API fastfft_status fastfft_set_output_dtype(fastfft_handle h, int dtype)
  * overflow).  The output buffer then holds ReturnFwdOutputMemorySize() / 2 complex values of
  * that type.  No reference counterpart (the reference's spectra are FP32). */
 FASTFFT_API fastfft_status fastfft_set_spectrum_output(fastfft_handle h, int dtype, float scale);
+/* Rotationally averaged power of a square 2D half spectrum `spectrum` (complex64, the [kx][ky]
+ * layout FwdFFT writes for an n x n transform): power[r] = mean |S|^2 over the elements of the
+ * full spectrum at radius r = floor(sqrt(kx^2 + ky^2)) (signed ky, frequency-index units),
+ * r = 0 .. n_bins - 1, the last bin also holding every larger radius; n_bins floats on the
+ * device.  Uses a small work array of the plan (allocated on first use).  No reference
+ * counterpart. */
+FASTFFT_API fastfft_status fastfft_radial_power(fastfft_handle h, const void* spectrum, int n, float* power,
+                                                int n_bins);
+/* out = in x filter[r] for every element of a square 2D half spectrum (complex64 in, radius r
+ * as in fastfft_radial_power, n_bins filter factors on the device): a band-pass, or whitening
+ * with filter = 1 / sqrt(power).  `out` is written in the plan's spectrum storage and scale
+ * (fastfft_set_spectrum_output); in place (out == in) only with complex64 storage.  No
+ * reference counterpart. */
+FASTFFT_API fastfft_status fastfft_apply_radial_filter(fastfft_handle h, const void* in, void* out, int n,
+                                                       const float* filter, int n_bins);
 
 /* FwdFFT(input, output, pre_op, intra_op) (FastFFT.h:165-170, FastFFT.cu:263-277).
  * Ops may be NULL (NOOP).  Output: complex64 spectrum [kz][kx][ky]. */

@@ -316,3 +316,36 @@ def image_spectrum_fp32(img: np.ndarray) -> np.ndarray:
 
 def cpu_workers() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+# ---------------------------------------------------------------------------
+# Radial operations on square 2D half spectra (image-spectrum preparation; no reference
+# counterpart: these define the semantics fastfft_radial_power / fastfft_apply_radial_filter
+# implement)
+# ---------------------------------------------------------------------------
+
+def radial_index(n: int, n_bins: int) -> np.ndarray:
+    """Bin of every element of an n x n half spectrum [kx][ky]: floor(sqrt(kx^2 + sy^2)) with
+    the signed ky (sy = ky - n above n/2), clipped to n_bins - 1."""
+    kx = np.arange(n // 2 + 1, dtype=np.int64)[:, None]
+    ky = np.arange(n, dtype=np.int64)[None, :]
+    sy = np.where(ky <= n // 2, ky, ky - n)
+    r = np.floor(np.sqrt((kx * kx + sy * sy).astype(np.float64))).astype(np.int64)
+    return np.minimum(r, n_bins - 1)
+
+
+def radial_power(spec: np.ndarray, n: int, n_bins: int) -> np.ndarray:
+    """Mean |S|^2 per radius over the full spectrum (columns 0 < kx < n/2 count twice)."""
+    s = np.asarray(spec).reshape(n // 2 + 1, n)
+    idx = radial_index(n, n_bins)
+    w = np.full((n // 2 + 1, 1), 2.0)
+    w[0] = w[-1] = 1.0
+    w = np.broadcast_to(w, s.shape)
+    sums = np.bincount(idx.ravel(), weights=(w * np.abs(s) ** 2).ravel(), minlength=n_bins)
+    wts = np.bincount(idx.ravel(), weights=w.ravel(), minlength=n_bins)
+    return np.where(wts > 0, sums / np.where(wts > 0, wts, 1), 0.0)
+
+
+def radial_filter(spec: np.ndarray, n: int, filt: np.ndarray, scale: float = 1.0) -> np.ndarray:
+    s = np.asarray(spec).reshape(n // 2 + 1, n)
+    return s * (np.asarray(filt, dtype=np.float64)[radial_index(n, len(filt))] * scale)
