@@ -141,3 +141,17 @@ def test_spectrum_output_setting_is_validated():
     assert lib.fastfft_set_spectrum_output(ft._h, C.DTYPE_C32H, 0.0) == C.ERR_INVALID_ARGUMENT   # zero
     assert lib.fastfft_set_spectrum_output(ft._h, C.DTYPE_C32H, float("nan")) == C.ERR_INVALID_ARGUMENT
     assert lib.fastfft_set_spectrum_output(None, C.DTYPE_C64, 1.0) == C.ERR_INVALID_ARGUMENT
+
+
+def test_radial_operations_validate_arguments():
+    ft = new()
+    lib = C.lib()
+    assert lib.fastfft_radial_power(None, 0x1000, 64, 0x2000, 10) == C.ERR_INVALID_ARGUMENT
+    assert lib.fastfft_radial_power(ft._h, None, 64, 0x2000, 10) == C.ERR_INVALID_ARGUMENT
+    assert lib.fastfft_radial_power(ft._h, 0x1000, 63, 0x2000, 10) == C.ERR_INVALID_DIMS      # odd n
+    assert lib.fastfft_radial_power(ft._h, 0x1000, 64, 0x2000, 0) == C.ERR_INVALID_ARGUMENT   # no bins
+    assert lib.fastfft_apply_radial_filter(ft._h, 0x1000, None, 64, 0x2000, 10) == C.ERR_INVALID_ARGUMENT
+    assert lib.fastfft_apply_radial_filter(ft._h, 0x1000, 0x3000, 16384, 0x2000, 10) == C.ERR_INVALID_DIMS
+    ft.SetSpectrumOutput("complex32", 1.0)
+    # in place needs complex64 storage
+    assert lib.fastfft_apply_radial_filter(ft._h, 0x1000, 0x1000, 64, 0x2000, 10) == C.ERR_INVALID_ARGUMENT
