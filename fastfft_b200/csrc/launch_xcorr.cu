@@ -7,12 +7,17 @@ namespace ffb {
 // dynamic shared memory available to one block (227 KB, less a little static shared memory)
 constexpr int kMaxDynSmem = 227 * 1024 - 1024;
 
+template <int N>
+constexpr int xcorr_fpb() {
+    return FftShape<N>::T >= kXcorrBlockThreads ? 1 : kXcorrBlockThreads / FftShape<N>::T;
+}
+
 template <int N, class ImgC>
 static cudaError_t xcorr_v2_impl(const XcorrColArgs& a, cudaStream_t st) {
     if constexpr (N > 4096) {
         return cudaErrorInvalidValue;
     } else {
-        constexpr int FPB = col_fpb<N>();
+        constexpr int FPB = xcorr_fpb<N>();
         using SM = XcorrSmem<N, ImgC, FPB>;
         if (a.n_batch < 1 || a.n_batch > kMaxBatch || a.n_cols < 1) return cudaErrorInvalidValue;
         if (a.tpb < 1 || a.tpb > a.n_batch) return cudaErrorInvalidValue;
@@ -46,7 +51,7 @@ cudaError_t launch_xcorr_cols(int n, int img_dtype, const XcorrColArgs& a, cudaS
 size_t xcorr_cols_smem(int n, int img_dtype, int L, int n_batch) {
     if (is_3p_size(n)) return xcorr3_smem(n, img_dtype, L, n_batch);
     const int isz = img_dtype == 3 ? 8 : 4;
-    const int fpb = (n / 16) >= 256 ? 1 : 256 / (n / 16);
+    const int fpb = (n / 16) >= kXcorrBlockThreads ? 1 : kXcorrBlockThreads / (n / 16);
     const size_t img = ((size_t)n * isz + 127) & ~(size_t)127;
     const size_t smem_fft = (size_t)(((n + n / 16) + 15) / 16) * 16 + 4;  // FftShape::SMEM_PAD
     const size_t xch = (size_t)fpb * 2 * smem_fft * 8;                    // double-buffered groups
