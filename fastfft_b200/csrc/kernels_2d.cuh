@@ -318,7 +318,7 @@ __device__ __forceinline__ unsigned long long peak_key(float v, unsigned int ind
 }
 
 template <int N, class OutT, int FPB>
-__global__ void __launch_bounds__(FftShape<N>::T * FPB)
+__global__ void __launch_bounds__(FftShape<N>::T * FPB, (FftShape<N>::T * FPB <= 256) ? 4 : 2)
 c2r_rows_kernel(RowInvArgs a) {
     using S = FftShape<N>;
     constexpr int T = S::T;

@@ -32,6 +32,13 @@ template <int N>
 constexpr int row_fpb() {
     return FftShape<N>::T >= 512 ? 1 : 512 / FftShape<N>::T;
 }
+// Row C2R below N = 4096: 256-thread blocks, four per SM (64 registers); measured on B200 in
+// the batched correlation: 0.90 instead of 0.99 us per template at 1024^2, 0.20 instead of 0.22
+// at 256^2.  At 4096 (the image preparation and the size-N path) the 512-thread blocks stay.
+template <int N>
+constexpr int c2r_fpb() {
+    return N >= 4096 ? row_fpb<N>() : (FftShape<N>::T >= 256 ? 1 : 256 / FftShape<N>::T);
+}
 template <int N>
 constexpr int col_fpb() {
     return FftShape<N>::T >= 256 ? 1 : 256 / FftShape<N>::T;

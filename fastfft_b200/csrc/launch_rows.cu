@@ -36,7 +36,7 @@ cudaError_t launch_r2c_rows(int n, int in_dtype, const RowFwdArgs& a, cudaStream
 
 template <int N, class OutT>
 static cudaError_t c2r_impl(const RowInvArgs& a, cudaStream_t st) {
-    constexpr int FPB = row_fpb<N>();
+    constexpr int FPB = c2r_fpb<N>();
     constexpr int THREADS = FftShape<N>::T * FPB;
     const size_t smem = (size_t)FftGroup<N, FPB, false>::BYTES;
     static std::atomic<unsigned long long> mask{0};
