@@ -117,7 +117,7 @@ __device__ __forceinline__ long long input_row(int r, int rows_y, int rows_z) {
 }
 
 template <int N, class InT, int FPB>
-__global__ void __launch_bounds__(FftShape<N>::T * FPB)
+__global__ void __launch_bounds__(FftShape<N>::T * FPB, (FftShape<N>::T * FPB <= 256) ? 4 : 2)
 r2c_rows_kernel(RowFwdArgs a) {
     using S = FftShape<N>;
     constexpr int T = S::T;

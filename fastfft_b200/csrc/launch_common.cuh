@@ -39,6 +39,12 @@ template <int N>
 constexpr int c2r_fpb() {
     return N >= 4096 ? row_fpb<N>() : (FftShape<N>::T >= 256 ? 1 : 256 / FftShape<N>::T);
 }
+// Row R2C likewise: 256-thread blocks below 4096 (0.81 instead of 0.85 us per template at
+// 1024^2, 0.24 instead of 0.26 at 256^2).
+template <int N>
+constexpr int r2c_fpb() {
+    return N >= 4096 ? row_fpb<N>() : (FftShape<N>::T >= 256 ? 1 : 256 / FftShape<N>::T);
+}
 template <int N>
 constexpr int col_fpb() {
     return FftShape<N>::T >= 256 ? 1 : 256 / FftShape<N>::T;

@@ -5,7 +5,7 @@ namespace ffb {
 
 template <int N, class InT>
 static cudaError_t r2c_impl(const RowFwdArgs& a, cudaStream_t st) {
-    constexpr int FPB = row_fpb<N>();
+    constexpr int FPB = r2c_fpb<N>();
     constexpr int THREADS = FftShape<N>::T * FPB;
     const size_t smem = (size_t)FftGroup<N, FPB, false>::BYTES;
     static std::atomic<unsigned long long> mask{0};
