@@ -17,6 +17,13 @@
 
 namespace ffb {
 
+// Resident threads per SM the register budget of the column passes (batched and single) is
+// sized for: 384 (168 registers), as 4 blocks of one 1536-point FFT (96 threads) each.  Small
+// blocks beat 2 blocks of 2 FFTs (named barriers per FFT) on B200: 5.66 instead of 5.94 us per
+// template at 1536 points in the batched pass, 1.41 instead of 1.58 at 768; a budget of 576
+// threads (96 registers) spills and loses at 1536.
+constexpr int kXcorr3SmThreads = 384;
+
 // ---------------------------------------------------------------------------
 // Row R2C (forward)
 // ---------------------------------------------------------------------------
@@ -243,7 +250,8 @@ c2r3_rows_kernel(RowInvArgs a) {
 // ---------------------------------------------------------------------------
 // OutC: storage type of the forward spectrum (FWD mode; the other modes write float2)
 template <int P, int MODE, class InC, class ImgC, int FPB, class OutC = float2>
-__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, (Fft3Shape<P>::T * FPB <= 256) ? 2 : 1)
+__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, Fft3Shape<P>::T * FPB < kXcorr3SmThreads
+                                                             ? kXcorr3SmThreads / (Fft3Shape<P>::T * FPB) : 1)
 cols3_kernel(ColArgs a) {
     using S3 = Fft3Shape<P>;
     constexpr int T = S3::T;
@@ -339,11 +347,6 @@ struct Xcorr3Smem {
     static __host__ __device__ constexpr int total(int L, int nb) { return bar_off(L, nb) + 16; }
 };
 
-// Resident threads per SM the register budget is sized for: 384 (168 registers), as 4 blocks
-// of one 1536-point FFT (96 threads) each.  Small blocks beat 2 blocks of 2 FFTs (named
-// barriers per FFT) on B200: 5.66 instead of 5.94 us per template at 1536 points, 1.41
-// instead of 1.58 at 768; a budget of 576 threads (96 registers) spills and loses at 1536.
-constexpr int kXcorr3SmThreads = 384;
 
 // TC: the sub-FFTs' radix-16 passes on the tensor cores in BF16 split precision (fft_tc.cuh;
 // P = 512 only, where a sub-FFT is one warp)
