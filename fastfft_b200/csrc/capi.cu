@@ -38,10 +38,11 @@ using namespace ffb;
 #endif
 
 // templates that one block of the fused column pass stages for a launch of n at column
-// length my; at 1536 (= 3 * 512) six per block measured best on B200 (5.37 instead of 5.47
-// us per template for that pass with 64 per launch; 4, 5 and 8 were slower)
+// length my; measured best on B200 with 64 per launch: six at 1536 (= 3 * 512; 5.37 instead of
+// 5.47 us per template for that pass; 4, 5 and 8 were slower), four at 1024 (1.99 instead of
+// 2.06; 6 and 16 were slower), eight elsewhere (at 256: 0.23 against 0.29 with four)
 static inline int xcorr_tpb(int n, long long my) {
-    const int per_block = (FFB_XCORR_TPB == 8 && my == 3 * 512) ? 6 : FFB_XCORR_TPB;
+    const int per_block = FFB_XCORR_TPB != 8 ? FFB_XCORR_TPB : my == 3 * 512 ? 6 : my == 1024 ? 4 : 8;
     return per_block > 0 && n > per_block ? per_block : n;
 }
 
