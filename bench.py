@@ -16,15 +16,24 @@ every retained lag reads image pixels < 1407).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank runs the same work on its own GPU (templates shard across
-GPUs, no collective in the data path; weak scaling); the elapsed device time is the max
-over ranks.  --impl reference times the host CPU implementation of the same transform
-(the FP32 restatement in oracle/, multithreaded pocketfft) on rank 0.
+At least K steps are timed, more when K steps would take under --min-seconds (default 1 s,
+so that the clocks are sampled several times); "steps" in the output is the number timed.
+Under torchrun each rank runs the same work on its own GPU (templates shard across GPUs,
+no collective in the data path; weak scaling); the elapsed device time is the max over
+ranks.  --impl reference times the host CPU implementation of the same transform (the FP32
+restatement in oracle/, multithreaded pocketfft) on rank 0.
+
+Besides the headline line's own keys, the JSON line carries the other workload families
+(64^2 -> 512^2 round trip; 64^3 -> 256^3 forward with the central 128^3 inverse; the
+uneven 1024-template batch; FP16/BF16 storage with and without the tensor-core DFT) and
+the cuFFT comparators (full size and the same reduced size), each with its accuracy
+against the FP64 oracle.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -42,11 +51,14 @@ UNIT = "templates/s"
 N, L, W = 4096, 384, 1024
 TEMPLATES_PER_STEP = 64
 N_IMAGES = 3
-# compulsory HBM bytes per template: template read + full image spectrum read + window write
-ALG_BYTES_PER_TEMPLATE = L * L * 4 + (N // 2 + 1) * N * 8 + W * W * 4
+# Bytes per template of the size-4096 formulation (template read + full image spectrum read
+# + window write).  The path correlates at a reduced exact size, so this is an equivalence
+# figure, reported beside the roofline of the kernels as built.
+SIZE_N_BYTES_PER_TEMPLATE = L * L * 4 + (N // 2 + 1) * N * 8 + W * W * 4
 FALLBACK_HBM_GBS = 6650.0
 # FP32 CUDA-core peak: 148 SMs x 128 lanes x 2 flop (FMA) x clock
 FP32_FLOP_PER_CYCLE = 148 * 128 * 2
+PASS_NAMES = ["r2c_rows", "cols_xcorr", "c2r_rows"]
 
 
 def fft_flops(n):
@@ -63,6 +75,23 @@ def path_flops_per_template(corr, L_rows, W_rows):
     cols = (mx // 2 + 1) * 2 * fft_flops(my)
     c2r = (W_rows + 1) // 2 * fft_flops(mx)
     return [r2c, cols, c2r]
+
+
+def pass_bytes_per_template(corr, t_xy, w_xy, per_launch, n_per_call, t_size=4, img_size=8, n_full=N):
+    """Compulsory HBM bytes per template of each kernel as built, at correlation size corr:
+    every input read once and every output written once, the reduced image spectrum once per
+    launch (shared by the launch's templates) and the image preparation once per call.
+    Returns [r2c, cols, c2r, prep]."""
+    mx, my = corr
+    lx, ly = t_xy
+    wx, wy = w_xy
+    kx = mx // 2 + 1
+    r2c = lx * ly * t_size + kx * ly * 8
+    cols = kx * ly * 8 + kx * my * 8 / per_launch + kx * wy * 8
+    c2r = kx * wy * 8 + wx * wy * 4
+    nk = n_full // 2 + 1
+    prep = (nk * n_full * img_size + 2 * nk * my * 8 + 2 * my * mx * 4 + 3 * kx * my * 8) / n_per_call
+    return [r2c, cols, c2r, prep]
 
 
 def config(templates_per_step, corr_size=None, per_launch=None):
@@ -89,24 +118,28 @@ def measured_hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-PROFILE_DOMINANT = os.path.join("profiles", "xcorr3_cols_batched_1536_template384_window1024.md")
+# committed ncu summary with the DRAM bytes per template of the three template kernels
+PROFILE_TRAFFIC = os.path.join("profiles", "traffic_bench_xcorr_1536_template384_window1024.md")
 
 
-def ncu_traffic_per_template():
-    """DRAM bytes (read + write) per template of the batched fused column kernel, from the
-    committed ncu summary of that kernel (one launch over a group of templates)."""
-    p = os.path.join(ROOT, PROFILE_DOMINANT)
+def profile_figures(rel_path):
+    """`key: value` lines of a committed ncu summary (numbers only)."""
+    out = {}
     try:
-        for line in open(p):
-            if line.startswith("traffic_bytes_per_template:"):
-                return int(line.split(":")[1].strip())
+        for line in open(os.path.join(ROOT, rel_path)):
+            if ":" in line and not line.startswith(("|", " ", "#")):
+                k, v = line.split(":", 1)
+                try:
+                    out[k.strip()] = float(v.strip())
+                except ValueError:
+                    pass
     except OSError:
         pass
-    return None
+    return out
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a timed region."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -149,13 +182,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def smi_index(local):
+    """nvidia-smi index of this rank's GPU (CUDA_VISIBLE_DEVICES maps local ordinals)."""
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    parts = [p.strip() for p in vis.split(",") if p.strip()]
+    if parts and local < len(parts) and parts[local].isdigit():
+        return int(parts[local])
+    return local
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
-        import torch.distributed as dist
         import datetime
+
+        import torch.distributed as dist
 
         backend = "nccl" if os.environ.get("FASTFFT_BENCH_BACKEND", "nccl") == "nccl" else "gloo"
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
@@ -177,6 +220,25 @@ def max_over_ranks(world, value, torch, device):
     t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def event_ms(torch, fn, reps):
+    """Device time of reps calls of fn on the current stream (CUDA events, synchronised)."""
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def reps_for(torch, fn, min_seconds, at_least=3):
+    """Number of calls of fn that lasts at least min_seconds (from a short timed sample)."""
+    sample = max(at_least, 5)
+    per = event_ms(torch, fn, sample) / sample * 1e-3
+    return max(at_least, int(math.ceil(min_seconds / max(per, 1e-7))))
 
 
 # ---------------------------------------------------------------------------
@@ -233,29 +295,37 @@ UNEVEN_N_TEMPLATES = 1024
 UNEVEN_WINDOW = 512
 
 
-def run_uneven(dev, image_f32, storage="float32", reps=5):
+def oracle_window(t_padded, t_xy, spec, w_xy, workers):
+    """FP64 size-4096 correlation of one template (oracle), the W x W window as (y, x)."""
+    from oracle import fastfft_oracle as O
+
+    fin, iout = (t_xy[0], t_xy[1], 1), (w_xy[0], w_xy[1], 1)
+    p = O.Plan(fin, (N, N, 1), (N, N, 1), iout)
+    return O.real_from_padded(O.fwd_image_inv(t_padded, spec, p, out_dtype=np.float64, workers=workers), iout)[0]
+
+
+def run_uneven(dev, image_f32, storage, local, min_seconds, check=True):
     """1024 templates with edges drawn uniformly from {128,192,256,384} (N(0,1), seeded),
     zero-padded to 4096^2, correlated against one resident 4096^2 image spectrum, cropped
     to 512^2 windows.  The whole batch is captured once in a CUDA graph and replayed.
     storage "bfloat16": templates and image spectrum stored in BF16 (image scaled by 1/4096
-    before rounding), arithmetic in FP32."""
+    before rounding), arithmetic in FP32.  Accuracy: the first template of every size
+    against the FP64 oracle of the stored inputs."""
     import torch
 
     import fastfft_b200 as F
     from fastfft_b200.autotune import tune
+    from oracle import fastfft_oracle as O
 
     rng = np.random.default_rng(20261203 + 5)
     edges = rng.choice(UNEVEN_SIZES, size=UNEVEN_N_TEMPLATES)
-    L, W = max(UNEVEN_SIZES), UNEVEN_WINDOW
+    Lmax, Wu = max(UNEVEN_SIZES), UNEVEN_WINDOW
     tdt = torch.float32 if storage == "float32" else torch.bfloat16
     ft = F.FourierTransformer(input_dtype=storage, image_dtype="complex64" if storage == "float32" else "complex_bf16")
-    ft.SetForwardFFTPlan(L, L, 1, N, N, 1)
-    ft.SetInverseFFTPlan(N, N, 1, W, W, 1)
+    ft.SetForwardFFTPlan(Lmax, Lmax, 1, N, N, 1)
+    ft.SetInverseFFTPlan(N, N, 1, Wu, Wu, 1)
     ft.SetOutputDtype("float32")
-    if storage == "float32":
-        image = image_f32
-    else:
-        image = (image_f32 * (1.0 / N)).to(tdt)
+    image = image_f32 if storage == "float32" else (image_f32 * (1.0 / N)).to(tdt)
     gen = torch.Generator(device=dev)
     gen.manual_seed(20261203 + 6)
     ins, sizes = [], []
@@ -276,28 +346,71 @@ def run_uneven(dev, image_f32, storage="float32", reps=5):
     with torch.cuda.graph(graph):
         ft.FwdImageInvFFTManySized(ins, sizes, image, outs)
     graph.replay()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
-        graph.replay()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
+    reps = reps_for(torch, graph.replay, min_seconds)
+    clocks = ClockSampler(smi_index(local))
+    clocks.start()
+    ms = event_ms(torch, graph.replay, reps) / reps
+    clk = clocks.stop()
     del graph
-    return {"workload": "1024 templates, edges uniform in {128,192,256,384}, zero-padded to 4096^2, one resident "
-                        "4096^2 image spectrum, 512^2 windows; the whole batch is one CUDA graph launch",
-            "storage": storage, "value": UNEVEN_N_TEMPLATES / (ms * 1e-3), "unit": UNIT, "ms_per_batch": ms,
-            "correlation_size": list(ft.CorrelationSize()), "templates_per_launch": per_launch,
-            "template_edge_counts": {str(k): int((edges == k).sum()) for k in UNEVEN_SIZES}}
+    peak, _ = measured_hbm_peak()
+    # compulsory bytes of the kernels as built, per class (correlation size of each class)
+    img_size = 8 if storage == "float32" else 4
+    t_size = 4 if storage == "float32" else 2
+    total_bytes = 0.0
+    counts = {int(k): int((edges == k).sum()) for k in UNEVEN_SIZES}
+    mean_size_n = 0.0
+    for e, cnt in counts.items():
+        m = corr_size_for(e, Wu)
+        b = pass_bytes_per_template((m, m), (e, e), (Wu, Wu), per_launch, cnt, t_size=t_size, img_size=img_size)
+        total_bytes += cnt * sum(b)
+        mean_size_n += cnt * (e * e * t_size + (N // 2 + 1) * N * img_size + Wu * Wu * 4)
+    res = {"workload": "1024 templates, edges uniform in {128,192,256,384}, zero-padded to 4096^2, one resident "
+                       "4096^2 image spectrum, 512^2 windows; the whole batch is one CUDA graph launch",
+           "storage": storage, "value": UNEVEN_N_TEMPLATES / (ms * 1e-3), "unit": UNIT, "ms_per_batch": ms,
+           "timed_batches": reps, "correlation_size": list(ft.CorrelationSize()), "templates_per_launch": per_launch,
+           "template_edge_counts": {str(k): v for k, v in counts.items()}, "clocks": clk,
+           "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak,
+                        "achieved": total_bytes / (ms * 1e-3) / 1e9,
+                        "frac": total_bytes / (ms * 1e-3) / 1e9 / peak,
+                        "algorithmic_bytes_per_batch": total_bytes,
+                        "how": "compulsory bytes of the kernels as built (each template's R2C, fused column pass "
+                               "and C2R at its size class's correlation size, the image preparation once per "
+                               "class) over the batch time",
+                        "equivalent_frac_vs_size_n_formulation": mean_size_n / (ms * 1e-3) / 1e9 / peak}}
+    if check:
+        spec = image.float().cpu().numpy().view(np.complex64).reshape(1, N // 2 + 1, N)
+        acc = {}
+        for e in UNEVEN_SIZES:
+            i = int(np.nonzero(edges == e)[0][0])
+            t_pad = ins[i].float().cpu().numpy()
+            ref = oracle_window(t_pad, (e, e), spec, (Wu, Wu), O.cpu_workers())
+            got = O.real_from_padded(out[i].cpu().numpy(), (Wu, Wu, 1))[0]
+            acc[str(e)] = {"template": i, "rel_l2_vs_fp64": O.rel_l2(got, ref), "rel_max_vs_fp64": O.rel_max(got, ref),
+                           "peak_index_exact": bool(O.peak(got)[0] == O.peak(ref)[0])}
+        res["accuracy"] = acc
+    return res
 
 
-def run_low_precision(dev, images_f32, templates_f32, storage, steps, warmup=3):
+def corr_size_for(edge, window):
+    """Shortest supported exact correlation length >= edge + window - 1 (power of two or 3 * 2^k,
+    2^k in [128, 2048]), capped at N."""
+    need = edge + window - 1
+    p2 = 1 << (need - 1).bit_length()
+    best = p2
+    for k in range(7, 12):
+        m = 3 << k
+        if need <= m < best:
+            best = m
+    return min(best, N)
+
+
+def run_storage(dev, images_f32, templates_f32, storage, steps, tc=False, warmup=3):
     """The headline workload with the templates and the image spectra stored in FP16 or
     BF16 (image spectra scaled by 1/4096 before rounding, the overflow guard), FP32
-    arithmetic and FP32 windows; same steps as the main leg (B templates per step, image
-    spectra rotating).  Returns the result and, for the accuracy check, template 0's window
-    with the dequantized template and image 0."""
+    arithmetic and FP32 windows, optionally with the fused column pass's radix-16 stages on
+    the tensor cores in split precision; same steps as the main leg (B templates per step,
+    image spectra rotating).  Returns the result and, for the accuracy check, template 0's
+    window with the dequantized template and image 0."""
     import torch
 
     import fastfft_b200 as F
@@ -308,6 +421,7 @@ def run_low_precision(dev, images_f32, templates_f32, storage, steps, warmup=3):
     ft.SetForwardFFTPlan(L, L, 1, N, N, 1)
     ft.SetInverseFFTPlan(N, N, 1, W, W, 1)
     ft.SetOutputDtype("float32")
+    ft.SetTensorCoreDFT(tc)
     B = templates_f32.shape[0]
     images = [(im * (1.0 / N)).to(tdt) for im in images_f32]
     templates = templates_f32.to(tdt)
@@ -315,22 +429,23 @@ def run_low_precision(dev, images_f32, templates_f32, storage, steps, warmup=3):
     ins = [templates[i] for i in range(B)]
     outs = [outputs[i] for i in range(B)]
     per_launch = tune(ft, ins, images[0], outs)
-    for i in range(warmup):
-        ft.FwdImageInvFFTMany(ins, images[i % len(images)], outs)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for i in range(steps):
-        ft.FwdImageInvFFTMany(ins, images[i % len(images)], outs)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    step_no = [0]
+
+    def step():
+        ft.FwdImageInvFFTMany(ins, images[step_no[0] % len(images)], outs)
+        step_no[0] += 1
+
+    for _ in range(warmup):
+        step()
+    ms = event_ms(torch, step, steps)
     ft.FwdImageInvFFTMany(ins[:1], images[0], outs[:1])
     torch.cuda.synchronize()
-    result = {"storage": storage, "value": steps * B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
-              "correlation_size": list(ft.CorrelationSize()), "templates_per_launch": per_launch,
-              "how": "templates and image spectra stored in " + storage + " (image spectra scaled by 1/4096), "
-                     "FP32 arithmetic, FP32 windows"}
+    how = ("templates and image spectra stored in " + storage + " (image spectra scaled by 1/4096), FP32 windows; "
+           + ("the fused column pass's 16-point DFTs as BF16 hi/lo tensor-core products with FP32 accumulation"
+              if tc else "FP32 arithmetic"))
+    result = {"storage": storage, "tensor_core_dft": bool(tc and ft.TensorCoreDFTActive()),
+              "value": steps * B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+              "correlation_size": list(ft.CorrelationSize()), "templates_per_launch": per_launch, "how": how}
     check = {"window": outputs[0].cpu().numpy(), "template": templates[0].float().cpu().numpy(),
              "image": images[0].float().cpu().numpy()}
     return result, check
@@ -354,24 +469,206 @@ def run_tensor_core(dev, images, templates, steps, warmup=3):
     ins = [templates[i] for i in range(B)]
     outs = [outputs[i] for i in range(B)]
     per_launch = tune(ft, ins, images[0], outs)
-    for i in range(warmup):
-        ft.FwdImageInvFFTMany(ins, images[i % len(images)], outs)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for i in range(steps):
-        ft.FwdImageInvFFTMany(ins, images[i % len(images)], outs)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    step_no = [0]
+
+    def step():
+        ft.FwdImageInvFFTMany(ins, images[step_no[0] % len(images)], outs)
+        step_no[0] += 1
+
+    for _ in range(warmup):
+        step()
+    ms = event_ms(torch, step, steps)
     ft.FwdImageInvFFTMany(ins[:1], images[0], outs[:1])
     torch.cuda.synchronize()
-    result = {"value": steps * B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
+    result = {"value": steps * B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
               "active": ft.TensorCoreDFTActive(), "correlation_size": list(ft.CorrelationSize()),
               "templates_per_launch": per_launch,
               "how": "FP32 storage; the fused column pass's 16-point DFTs as BF16 hi/lo matrix products "
-                     "(mma.sync m16n8k16, FP32 accumulation), everything else FP32"}
+                     "(FP32 accumulation), everything else FP32"}
     return result, outputs[0].cpu().numpy()
+
+
+# ---------------------------------------------------------------------------
+# The other two workload families: 2D round trip (64^2 -> 512^2) and 3D (64^3 -> 256^3)
+# ---------------------------------------------------------------------------
+def run_round_trip_2d(dev, local, min_seconds):
+    """64x64 N(0,1) at the origin of a 512^2 R2C (FwdFFT), then the 512^2 C2R of that
+    spectrum (InvFFT), batch 1.  48 independent buffer sets rotate (152 MB > L2); the
+    round trips are replayed from a CUDA graph (one graph of 48 round trips), so the time
+    is the device time of the launches, not Python's launch overhead."""
+    import torch
+
+    import fastfft_b200 as F
+    from oracle import fastfft_oracle as O
+
+    sets = 48
+    ft = F.FourierTransformer()
+    ft.SetForwardFFTPlan(64, 64, 1, 512, 512, 1)
+    ft.SetInverseFFTPlan(512, 512, 1, 512, 512, 1)
+    rng = np.random.default_rng(O.SEED_BASE + 1)
+    x = rng.standard_normal((64, 64)).astype(np.float32)
+    xin = torch.from_numpy(O.real_to_padded(x, (64, 64, 1))).to(dev)
+    ins = [xin.clone() for _ in range(sets)]
+    specs = [torch.empty(ft.ReturnFwdOutputMemorySize(), device=dev) for _ in range(sets)]
+    outs = [torch.empty(ft.ReturnInvOutputMemorySize(), device=dev) for _ in range(sets)]
+
+    def all_sets():
+        for i in range(sets):
+            ft.FwdFFT(ins[i], specs[i])
+            ft.InvFFT(specs[i], outs[i])
+
+    all_sets()
+    all_sets()
+    torch.cuda.synchronize()
+    eager_ms = event_ms(torch, all_sets, 3) / (3 * sets)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        all_sets()
+    graph.replay()
+    reps = reps_for(torch, graph.replay, min_seconds)
+    clocks = ClockSampler(smi_index(local))
+    clocks.start()
+    ms = event_ms(torch, graph.replay, reps) / (reps * sets)
+    clk = clocks.stop()
+    del graph
+    peak, _ = measured_hbm_peak()
+    fwd_bytes = 64 * 66 * 4 + 257 * 512 * 8
+    inv_bytes = 257 * 512 * 8 + 512 * 514 * 4
+    byts = fwd_bytes + inv_bytes
+    spec_ref = O.fwd(O.real_to_padded(x, (64, 64, 1)), (64, 64, 1), (512, 512, 1))
+    spec_got = specs[0].cpu().numpy().view(np.complex64).reshape(spec_ref.shape)
+    back_ref = O.real_from_padded(O.inv(spec_ref, (512, 512, 1), (512, 512, 1), out_dtype=np.float64), (512, 512, 1))
+    back_got = O.real_from_padded(outs[0].cpu().numpy(), (512, 512, 1))
+    return {"workload": "2D FP32 R2C 64^2 -> 512^2 (zero padding at the origin) then C2R 512^2 -> 512^2, batch 1",
+            "unit": "round trips/s", "value": 1e3 / ms, "us_per_round_trip": 1e3 * ms,
+            "us_per_round_trip_eager": 1e3 * eager_ms, "timed_round_trips": reps * sets, "clocks": clk,
+            "l2": f"{sets} buffer sets rotate ({sets * byts / 1e6:.0f} MB > 126 MB L2)",
+            "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak, "bytes_per_round_trip": byts,
+                         "achieved": byts / (ms * 1e-3) / 1e9, "frac": byts / (ms * 1e-3) / 1e9 / peak,
+                         "note": "launch-latency bound at this size (four kernels of a few microseconds)"},
+            "accuracy": {"spectrum_rel_l2_vs_fp64": O.rel_l2(spec_got, spec_ref),
+                         "round_trip_rel_l2_vs_fp64": O.rel_l2(back_got, back_ref),
+                         "round_trip_rel_max_vs_fp64": O.rel_max(back_got, back_ref)}}
+
+
+def run_3d(dev, local, min_seconds):
+    """64^3 N(0,1) zero-padded to a 256^3 R2C (FwdFFT), then the 256^3 C2R keeping the
+    central 128^3 (InvFFT with the output origin at 64^3), batch 1.  Three buffer sets
+    rotate (231 MB > L2); graph-replayed like the 2D round trip."""
+    import torch
+
+    import fastfft_b200 as F
+    from oracle import fastfft_oracle as O
+
+    sets = 3
+    ft = F.FourierTransformer(rank=3)
+    ft.SetForwardFFTPlan(64, 64, 64, 256, 256, 256)
+    ft.SetInverseFFTPlan(256, 256, 256, 128, 128, 128)
+    ft.SetInverseOutputOrigin(64, 64, 64)
+    rng = np.random.default_rng(O.SEED_BASE + 3)
+    x = rng.standard_normal((64, 64, 64)).astype(np.float32)
+    xin = torch.from_numpy(O.real_to_padded(x, (64, 64, 64))).to(dev)
+    ins = [xin.clone() for _ in range(sets)]
+    specs = [torch.empty(ft.ReturnFwdOutputMemorySize(), device=dev) for _ in range(sets)]
+    outs = [torch.empty(ft.ReturnInvOutputMemorySize(), device=dev) for _ in range(sets)]
+
+    def all_sets():
+        for i in range(sets):
+            ft.FwdFFT(ins[i], specs[i])
+            ft.InvFFT(specs[i], outs[i])
+
+    all_sets()
+    all_sets()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        all_sets()
+    graph.replay()
+    reps = reps_for(torch, graph.replay, min_seconds)
+    clocks = ClockSampler(smi_index(local))
+    clocks.start()
+    ms = event_ms(torch, graph.replay, reps) / (reps * sets)
+    clk = clocks.stop()
+    del graph
+    # passes timed separately (forward alone) for the per-direction figures
+    fwd_ms = event_ms(torch, lambda: [ft.FwdFFT(ins[i], specs[i]) for i in range(sets)], 10) / (10 * sets)
+    peak, _ = measured_hbm_peak()
+    fwd_bytes = 64 * 66 * 64 * 4 + 129 * 256 * 256 * 8
+    inv_bytes = 129 * 256 * 256 * 8 + 128 * 130 * 128 * 4
+    byts = fwd_bytes + inv_bytes
+    set_bytes = 64 * 66 * 64 * 4 + 129 * 256 * 256 * 8 + 128 * 130 * 128 * 4
+    spec_ref = O.fwd(O.real_to_padded(x, (64, 64, 64)), (64, 64, 64), (256, 256, 256), workers=O.cpu_workers())
+    spec_got = specs[0].cpu().numpy().view(np.complex64).reshape(spec_ref.shape)
+    back_ref = O.real_from_padded(O.inv(spec_ref, (256, 256, 256), (128, 128, 128), out_dtype=np.float64,
+                                        workers=O.cpu_workers(), origin=(64, 64, 64)), (128, 128, 128))
+    back_got = O.real_from_padded(outs[0].cpu().numpy(), (128, 128, 128))
+    return {"workload": "3D FP32 R2C 64^3 -> 256^3 (zero padding at the origin) then C2R 256^3 keeping the central "
+                        "128^3, batch 1",
+            "unit": "round trips/s", "value": 1e3 / ms, "us_per_round_trip": 1e3 * ms, "us_forward": 1e3 * fwd_ms,
+            "timed_round_trips": reps * sets, "clocks": clk,
+            "l2": f"{sets} buffer sets rotate ({sets * set_bytes / 1e6:.0f} MB > 126 MB L2)",
+            "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak, "bytes_per_round_trip": byts,
+                         "achieved": byts / (ms * 1e-3) / 1e9, "frac": byts / (ms * 1e-3) / 1e9 / peak,
+                         "forward_frac": fwd_bytes / (fwd_ms * 1e-3) / 1e9 / peak},
+            "accuracy": {"spectrum_rel_l2_vs_fp64": O.rel_l2(spec_got, spec_ref),
+                         "window_rel_l2_vs_fp64": O.rel_l2(back_got, back_ref),
+                         "window_rel_max_vs_fp64": O.rel_max(back_got, back_ref)}}
+
+
+# ---------------------------------------------------------------------------
+# cuFFT comparators (torch.fft): the size-4096 pad-then-transform and the same reduced size
+# ---------------------------------------------------------------------------
+def run_cufft(dev, images, templates, window0, corr, batch_full=16):
+    """torch.fft (cuFFT) pad-then-transform: (a) at 4096^2, batches of batch_full templates:
+    pad, rfft2, conj-multiply with the image spectrum, irfft2, crop; (b) at the reduced exact
+    size our path uses (corr): per step of the templates, the image crop's spectrum from the
+    4096^2 spectrum (irfft2 at 4096^2, crop, rfft2) and the batched correlation at that size.
+    Both scale like the reference (output = N^2 x correlation); (b)'s window is compared with
+    our window of template 0."""
+    import torch
+
+    B = templates.shape[0]
+    mx, my = corr
+    tv = templates.view(B, L, -1)[:, :, :L]
+    specs_c = [im.view(torch.complex64).view(N // 2 + 1, N).t() for im in images]   # [ky][kx]
+    pad_full = torch.zeros(batch_full, N, N, device=dev)
+    pad_red = torch.zeros(B, my, mx, device=dev)
+
+    def full_batch(i0):
+        pad_full[:, :L, :L] = tv[i0:i0 + batch_full]
+        s = torch.fft.rfft2(pad_full)
+        r = torch.fft.irfft2(torch.conj(s) * specs_c[0], s=(N, N))
+        return r[:, :W, :W].contiguous()
+
+    full_batch(0)
+    reps = 4
+    ms_full = event_ms(torch, lambda: full_batch(0), reps) / reps
+    step_no = [0]
+
+    def reduced_step():
+        spec = specs_c[step_no[0] % len(specs_c)]
+        step_no[0] += 1
+        img = torch.fft.irfft2(spec, s=(N, N))
+        spec_m = torch.fft.rfft2(img[:my, :mx]) * float(N * N)
+        pad_red[:, :L, :L] = tv
+        t_hat = torch.fft.rfft2(pad_red)
+        r = torch.fft.irfft2(torch.conj(t_hat) * spec_m, s=(my, mx))
+        return r[:, :W, :W].contiguous()
+
+    reduced_step()
+    reps = 10
+    ms_red = event_ms(torch, reduced_step, reps) / reps
+    step_no[0] = 0
+    win = reduced_step()[0].cpu().numpy()
+    ours = window0.reshape(W, -1)[:, :W]
+    rel = float(np.linalg.norm(win - ours) / np.linalg.norm(ours))
+    return {"full_size": {"value": batch_full / (ms_full * 1e-3), "unit": UNIT,
+                          "how": f"torch.fft (cuFFT), batches of {batch_full}: pad to 4096^2, rfft2, conj-multiply, "
+                                 "irfft2, crop to 1024^2"},
+            "reduced_size": {"value": B / (ms_red * 1e-3), "unit": UNIT, "correlation_size": [mx, my],
+                             "how": f"torch.fft (cuFFT), {B} templates per step: image crop spectrum (irfft2 4096^2, "
+                                    f"crop, rfft2 at {mx}x{my}) then pad, rfft2, conj-multiply, irfft2, crop",
+                             "rel_l2_vs_ours": rel}}
 
 
 # ---------------------------------------------------------------------------
@@ -424,17 +721,21 @@ def run_ours(args, world, rank, local):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    # steps timed: at least --steps, more if that would end before --min-seconds
+    steps = max(args.steps, reps_for(torch, step, args.min_seconds, at_least=1))
+    steps = int(max_over_ranks(world, float(steps), torch, dev))
+    calls_per_step = -(-B // max(per_launch, 1))
 
     # ---- timed region (device-resident inputs) ----
-    clocks = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    clocks = ClockSampler(smi_index(local))
     launches0 = ft.LaunchCount()
-    ft.ProfileStart(args.steps * B)
+    ft.ProfileStart(steps * calls_per_step + 1)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(world, torch)
     torch.cuda.synchronize()
     clocks.start()
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
     e1.record()
     torch.cuda.synchronize()
@@ -443,38 +744,61 @@ def run_ours(args, world, rank, local):
     pass_ms, n_calls = ft.ProfileStop()
     launches = ft.LaunchCount() - launches0
     ms = max_over_ranks(world, e0.elapsed_time(e1), torch, dev)
-    value = world * args.steps * B / (ms * 1e-3)
+    value = world * steps * B / (ms * 1e-3)
 
-    # dominant kernel: the fused column pass (pass 1); the others reported beside it.
-    # One profiled call covers one launch of each pass over a group of templates, so the
-    # per-template time of a pass is its summed launch time over the templates timed.
-    n_templates = args.steps * B
+    # Per-pass device time (CUDA events on the plan's stream around each launch); one
+    # profiled call covers one launch of each pass over a group of templates.
+    n_templates = steps * B
     per_pass_us = [1e3 * p / n_templates for p in pass_ms]
     dom = int(np.argmax(per_pass_us))
     peak, peak_kind = measured_hbm_peak()
-    achieved = ALG_BYTES_PER_TEMPLATE / (per_pass_us[dom] * 1e-6) / 1e9
-    traffic = ncu_traffic_per_template()
-    # The bytes above are the size-4096 formulation's; the path reads far less (it shares the
-    # reduced image spectrum across templates), so the HBM fraction can exceed 1.  Beside it,
-    # the FP32 fraction of the transforms actually run, at the clock sampled in the timed
-    # region (max clock if no sample).
     corr_now = ft.CorrelationSize()
+    alg = pass_bytes_per_template(corr_now, (L, L), (W, W), per_launch, B)
+    step_us = ms * 1e3 / n_templates
+    tmpl_per_launch = n_templates / max(n_calls, 1)
+    prof = profile_figures(PROFILE_TRAFFIC)
+    traffic_keys = ["r2c_traffic_bytes_per_template", "cols_traffic_bytes_per_template",
+                    "c2r_traffic_bytes_per_template"]
+    traffic = [prof.get(k) for k in traffic_keys]
+    achieved = alg[dom] / (per_pass_us[dom] * 1e-6) / 1e9
     flops = path_flops_per_template(corr_now, L, W)
-    compute = {"bound": "fp32", "unit": "TFLOP/s", "flop_convention": "5 n log2 n per complex n-FFT",
-               "flop_per_template": sum(flops), "flop_per_template_dominant": flops[dom],
-               "correlation_size": list(corr_now)}
     sm_mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
-    compute["peak"] = FP32_FLOP_PER_CYCLE * sm_mhz * 1e6 / 1e12
-    compute["peak_clock_mhz"] = sm_mhz
-    compute["achieved_dominant"] = flops[dom] / (per_pass_us[dom] * 1e-6) / 1e12
-    compute["frac_dominant"] = compute["achieved_dominant"] / compute["peak"]
-    compute["achieved_step"] = sum(flops) / (ms * 1e-3 / n_templates) / 1e12
-    compute["frac_step"] = compute["achieved_step"] / compute["peak"]
+    fp32_peak = FP32_FLOP_PER_CYCLE * sm_mhz * 1e6 / 1e12
+    roofline = {
+        "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_source": peak_kind,
+        "kernel": PASS_NAMES[dom],
+        "achieved": achieved, "frac": achieved / peak,
+        "traffic": traffic[dom] * tmpl_per_launch if traffic[dom] else None,
+        "algorithmic_bytes_per_launch": alg[dom] * tmpl_per_launch,
+        "templates_per_launch": tmpl_per_launch,
+        "how": "achieved = compulsory bytes of the dominant kernel as built (its template inputs, the reduced image "
+               "spectrum once per launch, its outputs) / its CUDA-event time; traffic = ncu DRAM bytes per launch "
+               "(" + PROFILE_TRAFFIC + ")",
+        "pass_us_per_template": per_pass_us,
+        "algorithmic_bytes_per_template": {"r2c": alg[0], "cols": alg[1], "c2r": alg[2], "image_prep": alg[3]},
+        "traffic_bytes_per_template": dict(zip(["r2c", "cols", "c2r"], traffic)),
+        "traffic_frac_dominant": (traffic[dom] / (per_pass_us[dom] * 1e-6) / 1e9 / peak) if traffic[dom] else None,
+        "pipeline_frac": sum(alg) / (step_us * 1e-6) / 1e9 / peak,
+        "pipeline_traffic_frac": (sum(traffic) / (step_us * 1e-6) / 1e9 / peak) if all(traffic) else None,
+        "equivalent_frac_vs_size_n_formulation": {
+            "bytes_per_template": SIZE_N_BYTES_PER_TEMPLATE,
+            "dominant": SIZE_N_BYTES_PER_TEMPLATE / (per_pass_us[dom] * 1e-6) / 1e9 / peak,
+            "step": SIZE_N_BYTES_PER_TEMPLATE / (step_us * 1e-6) / 1e9 / peak,
+            "note": "bytes the size-4096 formulation would have to move per template, over our time: the "
+                    "speed relative to that formulation at the HBM roofline, not a bandwidth"},
+        "compute": {"bound": "fp32", "unit": "TFLOP/s", "flop_convention": "5 n log2 n per complex n-FFT",
+                    "flop_per_template": sum(flops), "flop_per_template_dominant": flops[dom],
+                    "peak": fp32_peak, "peak_clock_mhz": sm_mhz,
+                    "achieved_dominant": flops[dom] / (per_pass_us[dom] * 1e-6) / 1e12,
+                    "frac_dominant": flops[dom] / (per_pass_us[dom] * 1e-6) / 1e12 / fp32_peak,
+                    "achieved_step": sum(flops) / (step_us * 1e-6) / 1e12,
+                    "frac_step": sum(flops) / (step_us * 1e-6) / 1e12 / fp32_peak},
+    }
 
     # ---- end to end: pinned host templates in, results back to pinned host ----
     # The windows (4.2 MB per template) come back over PCIe on a copy stream that overlaps
     # the next step's compute; a second buffer pair keeps the steps independent.
-    e2e_steps = max(2, min(args.steps, 10))
+    e2e_steps = max(2, min(steps, 10))
     h_in = torch.empty(B, n_in, dtype=torch.float32, pin_memory=True)
     h_in.copy_(templates.cpu())
     h_out = [torch.empty(B, n_out, dtype=torch.float32, pin_memory=True) for _ in range(2)]
@@ -549,9 +873,8 @@ def run_ours(args, world, rank, local):
 
     # the same through the fused maximum projection (a template search's per-pixel best
     # score and best template): each step searches its image with the step's templates and
-    # reads the W x W projection back (8 bytes per pixel per step, not per template)
-    # two projection buffers: step s searches into mips[s % 2] while the copy stream reads
-    # the previous step's projection back
+    # reads the W x W projection back (8 bytes per pixel per step, not per template);
+    # step s searches into mips[s % 2] while the copy stream reads the previous one back
     mips = [torch.zeros(W * W, dtype=torch.int64, device=dev) for _ in range(2)]
     h_mip = [torch.empty(W * W, dtype=torch.int64, pin_memory=True) for _ in range(2)]
     searched = [torch.cuda.Event() for _ in range(2)]
@@ -592,81 +915,72 @@ def run_ours(args, world, rank, local):
     mip_ms = max_over_ranks(world, f0.elapsed_time(f1), torch, dev)
     mip_value = world * e2e_steps * B / (mip_ms * 1e-3)
 
-    # ---- cuFFT pad-then-transform comparator (torch.fft) ----
+    # template 0's window against image 0 (accuracy check and the comparators' reference)
+    ft.FwdImageInvFFTMany(ins, images[0], outs)
+    torch.cuda.synchronize()
+    window0 = outputs[0].cpu().numpy()
+
+    extra = rank == 0 and not args.skip_uneven
+    # ---- cuFFT comparators (rank 0) ----
     cufft = None
     if rank == 0 and not args.skip_cufft:
-        spec_c = images[0].view(torch.complex64).view(N // 2 + 1, N).t()  # [ky][kx]
+        cufft = run_cufft(dev, images, templates, window0, corr_now)
+        strongest = max(cufft["full_size"]["value"], cufft["reduced_size"]["value"])
+        cufft["ours_over_strongest"] = value / world / strongest
 
-        def cufft_one(i):
-            p = torch.zeros(N, N, device=dev)
-            p[:L, :L] = templates[i].view(L, -1)[:, :L]
-            s = torch.fft.rfft2(p)
-            r = torch.fft.irfft2(torch.conj(s) * spec_c, s=(N, N))
-            return r[:W, :W].contiguous()
-
-        for i in range(3):
-            cufft_one(i)
-        torch.cuda.synchronize()
-        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 20
-        g0.record()
-        for i in range(reps):
-            cufft_one(i % B)
-        g1.record()
-        torch.cuda.synchronize()
-        cufft_v = reps / (g0.elapsed_time(g1) * 1e-3)
-        cufft = {"value": cufft_v, "unit": UNIT, "how": "torch.fft (cuFFT): pad, rfft2, conj-multiply, irfft2, crop",
-                 "ours_over_cufft": value / world / cufft_v}
+    # ---- the other workload families (rank 0) ----
+    round_trip_2d = run_round_trip_2d(dev, local, args.leg_seconds) if extra else None
+    volume_3d = run_3d(dev, local, args.leg_seconds) if extra else None
 
     # ---- uneven batch (rank 0): FP32 and BF16 storage ----
     uneven = None
-    if rank == 0 and not args.skip_uneven:
-        uneven = [run_uneven(dev, images[0], "float32"), run_uneven(dev, images[0], "bfloat16")]
+    if extra:
+        uneven = [run_uneven(dev, images[0], s, local, args.leg_seconds, check=not args.skip_cpu)
+                  for s in ("float32", "bfloat16")]
 
     # ---- the reference's plain API: one FwdImageInvFFT call per template (rank 0) ----
     plain = None
-    if rank == 0 and not args.skip_uneven:
+    if extra:
         plain = []
         for reuse in (False, True):
             single = F.FourierTransformer()
             single.SetForwardFFTPlan(L, L, 1, N, N, 1)
             single.SetInverseFFTPlan(N, N, 1, W, W, 1)
             single.SetImageReuse(reuse)
+            s_no = [0]
 
-            def one_step(s_no):
+            def one_step():
                 for i in range(B):
-                    single.FwdImageInvFFT(ins[i], images[s_no % N_IMAGES], outs[i])
+                    single.FwdImageInvFFT(ins[i], images[s_no[0] % N_IMAGES], outs[i])
+                s_no[0] += 1
 
-            for s_no in range(2):
-                one_step(s_no)
-            torch.cuda.synchronize()
+            one_step()
+            one_step()
             reps = 5
-            g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            g0.record()
-            for s_no in range(reps):
-                one_step(s_no)
-            g1.record()
-            torch.cuda.synchronize()
-            plain.append({"image_reuse": reuse, "value": reps * B / (g0.elapsed_time(g1) * 1e-3), "unit": UNIT,
+            plain.append({"image_reuse": reuse, "value": reps * B / (event_ms(torch, one_step, reps) * 1e-3),
+                          "unit": UNIT,
                           "correlation_size": list(single.CorrelationSize()) if reuse else [N, N],
                           "how": "one FwdImageInvFFT call per template, " + str(B) + " per image, images rotating"})
             del single
 
-    # ---- the headline workload with FP16 / BF16 storage (rank 0) ----
-    low = None
-    low_checks = {}
-    if rank == 0 and not args.skip_uneven:
-        low = []
+    # ---- the headline workload with FP16 / BF16 storage, without and with the tensor-core DFT ----
+    low, low_tc = None, None
+    checks = {}
+    if extra:
+        low, low_tc = [], []
         for storage in ("float16", "bfloat16"):
-            r, chk = run_low_precision(dev, images, templates, storage, args.steps)
+            r, chk = run_storage(dev, images, templates, storage, min(steps, 300))
             low.append(r)
-            low_checks[storage] = chk
+            checks[("low", storage)] = chk
+            r, chk = run_storage(dev, images, templates, storage, min(steps, 300), tc=True)
+            low_tc.append(r)
+            checks[("tc", storage)] = chk
     tensor_core = None
     tc_window = None
-    if rank == 0 and not args.skip_uneven:
-        tensor_core, tc_window = run_tensor_core(dev, images, templates, args.steps)
+    if extra:
+        tensor_core, tc_window = run_tensor_core(dev, images, templates, min(steps, 300))
 
-    # ---- CPU baseline (rank 0, one GPU) and accuracy check of one window ----
+    # ---- CPU baseline (rank 0, one GPU) and accuracy checks against the FP64 oracle ----
     cpu = None
     accuracy = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -683,50 +997,38 @@ def run_ours(args, world, rank, local):
         dt = time.perf_counter() - t0
         cpu = {"value": n_cpu / dt, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{n_cpu} templates (384^2 -> 4096^2 -> 1024^2, FP32 pocketfft, {cores} threads)"}
-        # accuracy of template 0 against the FP64 oracle
-        ft.FwdImageInvFFTMany(ins, images[0], outs)         # template 0's window against image 0
-        torch.cuda.synchronize()
         spec0 = images[0].cpu().numpy().view(np.complex64).reshape(1, N // 2 + 1, N)
-        plan = O.Plan((L, L, 1), (N, N, 1), (N, N, 1), (W, W, 1))
-        ref = O.real_from_padded(O.fwd_image_inv(templates[0].cpu().numpy(), spec0, plan, out_dtype=np.float64),
-                                 (W, W, 1))
-        got = O.real_from_padded(outputs[0].cpu().numpy(), (W, W, 1))
-        gi, _, _ = O.peak(got)
+        ref = oracle_window(templates[0].cpu().numpy(), (L, L), spec0, (W, W), cores)
+        got = O.real_from_padded(window0, (W, W, 1))[0]
+        gi = O.peak(got)[0]
         ri, rtop, margin = O.peak(ref)
         accuracy = {"rel_l2_vs_fp64": O.rel_l2(got, ref), "rel_max_vs_fp64": O.rel_max(got, ref),
                     "peak_index_exact": bool(gi == ri), "peak_margin_rel": margin / abs(rtop)}
         # low-precision storage: against the FP64 oracle of the dequantized template and image
-        # (the rounding of the stored inputs is the caller's choice; the path adds FP32 error
-        # only), and the peak index against the FP32 path's
-        for r in low or []:
-            chk = low_checks[r["storage"]]
-            spec_q = chk["image"].view(np.complex64).reshape(1, N // 2 + 1, N)
-            ref_q = O.real_from_padded(O.fwd_image_inv(chk["template"], spec_q, plan, out_dtype=np.float64), (W, W, 1))
-            got_q = O.real_from_padded(chk["window"], (W, W, 1))
-            r["accuracy"] = {"rel_l2_vs_fp64_of_stored_inputs": O.rel_l2(got_q, ref_q),
-                             "peak_index_equals_fp32_path": bool(O.peak(got_q)[0] == gi)}
+        # (the rounding of the stored inputs is the caller's choice; the path adds its own
+        # arithmetic error only), and the peak index against the FP32 path's
+        for kind, legs in (("low", low or []), ("tc", low_tc or [])):
+            for r in legs:
+                chk = checks[(kind, r["storage"])]
+                spec_q = chk["image"].view(np.complex64).reshape(1, N // 2 + 1, N)
+                ref_q = oracle_window(chk["template"], (L, L), spec_q, (W, W), cores)
+                got_q = O.real_from_padded(chk["window"], (W, W, 1))[0]
+                r["accuracy"] = {"rel_l2_vs_fp64_of_stored_inputs": O.rel_l2(got_q, ref_q),
+                                 "rel_max_vs_fp64_of_stored_inputs": O.rel_max(got_q, ref_q),
+                                 "peak_index_equals_fp32_path": bool(O.peak(got_q)[0] == gi),
+                                 "peak_index_exact": bool(O.peak(got_q)[0] == O.peak(ref_q)[0])}
         if tensor_core is not None:
-            got_tc = O.real_from_padded(tc_window, (W, W, 1))
+            got_tc = O.real_from_padded(tc_window, (W, W, 1))[0]
             tensor_core["accuracy"] = {"rel_l2_vs_fp64": O.rel_l2(got_tc, ref), "rel_max_vs_fp64": O.rel_max(got_tc, ref),
                                        "peak_index_equals_fp32_path": bool(O.peak(got_tc)[0] == gi)}
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config(B, corr_size, per_launch),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": ["r2c_rows", "cols_xcorr", "c2r_rows"][dom],
-                         "algorithmic_bytes_per_template": ALG_BYTES_PER_TEMPLATE,
-                         "templates_per_launch": n_templates / max(n_calls, 1),
-                         "algorithmic_bytes_per_launch": ALG_BYTES_PER_TEMPLATE * n_templates / max(n_calls, 1),
-                         "traffic_note": "traffic = ncu DRAM bytes (read + write) per template of the fused "
-                                         "column kernel, from " + PROFILE_DOMINANT + "; achieved and traffic are "
-                                         "both per template",
-                         "pass_us_per_template": per_pass_us,
-                         "pipeline_frac": ALG_BYTES_PER_TEMPLATE / (ms * 1e-3 / (args.steps * B)) / 1e9 / peak,
-                         "compute": compute},
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": ms / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config(B, corr_size, per_launch),
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": B * n_in * 4,
                     "d2h_bytes_per_step": B * n_out * 4, "steps": e2e_steps,
@@ -740,12 +1042,68 @@ def run_ours(args, world, rank, local):
                           "how": "FwdImageInvFFTManyPeaks: window max and argmax per template, windows not written"},
             "gpu_launches": launches,
             "clocks": clk,
-            "cufft_pad_then_transform": cufft,
+            "cufft": cufft,
             "accuracy": accuracy,
-            "uneven_batch": uneven, "low_precision_storage": low, "tensor_core_split": tensor_core,
-            "plain_api": plain,
+            "round_trip_2d": round_trip_2d, "volume_3d": volume_3d,
+            "uneven_batch": uneven, "low_precision_storage": low, "low_precision_tc": low_tc,
+            "tensor_core_split": tensor_core, "plain_api": plain,
         }
         print(json.dumps(line), flush=True)
+
+
+def run_profile_case(case, local):
+    """A small fixed workload for ncu captures (no timing, no checks): one warm-up call and
+    one profiled call.  "headline": 64 templates of 384^2 against one 4096^2 image spectrum,
+    1024^2 windows (the bench's step: image preparation, R2C, fused column pass, C2R);
+    "single": one FwdImageInvFFT call of that template at the size-4096 kernels;
+    "uneven": the 1024-template uneven batch's first 64 templates (FP32)."""
+    import torch
+
+    import fastfft_b200 as F
+    from fastfft_b200.workloads import blob_image, to_padded
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    prep = F.FourierTransformer()
+    prep.SetForwardFFTPlan(N, N, 1, N, N, 1)
+    prep.SetInverseFFTPlan(N, N, 1, N, N, 1)
+    x = torch.from_numpy(to_padded(blob_image(N))).to(dev)
+    spec = torch.empty(prep.ReturnFwdOutputMemorySize(), dtype=torch.float32, device=dev)
+    prep.FwdFFT(x, spec)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(20261203 + 1)
+    if case == "uneven":
+        rng = np.random.default_rng(20261203 + 5)
+        edges = rng.choice(UNEVEN_SIZES, size=64)
+        ft = F.FourierTransformer()
+        ft.SetForwardFFTPlan(max(UNEVEN_SIZES), max(UNEVEN_SIZES), 1, N, N, 1)
+        ft.SetInverseFFTPlan(N, N, 1, UNEVEN_WINDOW, UNEVEN_WINDOW, 1)
+        ins, sizes = [], []
+        for e in edges:
+            e = int(e)
+            t = torch.zeros(e, 2 * (e // 2 + 1), device=dev)
+            t[:, :e] = torch.randn(e, e, device=dev, generator=gen)
+            ins.append(t.view(-1))
+            sizes.append((e, e))
+        outs = [torch.empty(ft.ReturnInvOutputMemorySize(), device=dev) for _ in edges]
+        for _ in range(2):
+            ft.FwdImageInvFFTManySized(ins, sizes, spec, outs)
+    else:
+        ft = F.FourierTransformer()
+        ft.SetForwardFFTPlan(L, L, 1, N, N, 1)
+        ft.SetInverseFFTPlan(N, N, 1, W, W, 1)
+        B = 64 if case == "headline" else 1
+        templates = torch.zeros(B, ft.ReturnInputMemorySize(), device=dev)
+        templates.view(B, L, -1)[:, :, :L] = torch.randn(B, L, L, device=dev, generator=gen)
+        outputs = torch.empty(B, ft.ReturnInvOutputMemorySize(), device=dev)
+        for _ in range(2):
+            if case == "headline":
+                ft.SetTemplatesPerLaunch(64)
+                ft.FwdImageInvFFTMany([templates[i] for i in range(B)], spec, [outputs[i] for i in range(B)])
+            else:
+                ft.FwdImageInvFFT(templates[0], spec, outputs[0])
+    torch.cuda.synchronize()
+    print("profile case done:", case)
 
 
 def main():
@@ -755,11 +1113,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--templates-per-step", type=int, default=TEMPLATES_PER_STEP)
+    ap.add_argument("--min-seconds", type=float, default=1.0,
+                    help="the headline timed region lasts at least this long (more steps than --steps if needed)")
+    ap.add_argument("--leg-seconds", type=float, default=0.5, help="timed region of each secondary workload")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-cufft", action="store_true")
-    ap.add_argument("--skip-uneven", action="store_true")
+    ap.add_argument("--skip-uneven", action="store_true", help="skip the secondary workloads")
+    ap.add_argument("--profile-case", choices=["headline", "single", "uneven"],
+                    help="run one small fixed workload for an ncu capture and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        run_profile_case(args.profile_case, int(os.environ.get("LOCAL_RANK", "0")))
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()
     try:

@@ -35,8 +35,9 @@ namespace FastFFT {
 
 namespace KernelFunction {
 
-// Functor kinds (reference include/detail/functors.h).
-enum IKF_t { NOOP, CONJ_MUL, CONJ_MUL_THEN_SCALE, SCALE };
+// Functor kinds, with the reference's enumerator values (include/detail/concepts.h:22-25), so
+// that callers that store or cast them select the same functor.
+enum IKF_t { NOOP, SCALE, CONJ_MUL, CONJ_MUL_THEN_SCALE };
 
 template <typename T, int N_ARGS, IKF_t U, typename = void>
 struct my_functor {};

@@ -5,6 +5,14 @@
 
 #include "FastFFT.h"
 
+// the functor kinds keep the reference's enumerator values (include/detail/concepts.h:22-25)
+namespace KF = FastFFT::KernelFunction;
+static_assert(KF::NOOP == 0 && KF::SCALE == 1 && KF::CONJ_MUL == 2 && KF::CONJ_MUL_THEN_SCALE == 3,
+              "IKF_t values differ from the reference's");
+static_assert(int(KF::SCALE) == int(FASTFFT_OP_SCALE) && int(KF::CONJ_MUL) == int(FASTFFT_OP_CONJ_MUL) &&
+                  int(KF::CONJ_MUL_THEN_SCALE) == int(FASTFFT_OP_CONJ_MUL_THEN_SCALE),
+              "IKF_t values differ from the C ABI's op kinds");
+
 int main(int argc, char**) {
     FastFFT::FourierTransformer<float, float, float2, 2> ft;
     ft.SetForwardFFTPlan(384, 384, 1, 4096, 4096, 1, true);

@@ -62,3 +62,78 @@ def test_gather_over_two_gloo_ranks():
         assert v == [k * 1.5 for k in range(n_total)]
         assert i == [1000 + k for k in range(n_total)]
         assert t == 11.0
+
+
+# --- the sharded search on real per-rank results -------------------------------------
+# Each rank correlates only its shard_range() of the templates against its own copy of the
+# image spectrum (the oracle stands in for the GPU pass on CPU ranks), keeps (peak value,
+# peak index) per template, and gather_peaks() assembles the batch in template order; the
+# result must equal one rank searching every template.
+SEARCH_N, SEARCH_L, SEARCH_W, SEARCH_T = 128, 24, 48, 7
+
+
+def _search_inputs():
+    import numpy as np
+
+    from oracle import fastfft_oracle as O
+
+    img = O.gaussian_blob_image(SEARCH_N, n_blobs=3, seed=O.SEED_BASE + 31)
+    fout = (SEARCH_N, SEARCH_N, 1)
+    spec = O.fwd(O.real_to_padded(img, fout, dtype=np.float64), fout, fout)
+    rng = np.random.default_rng(O.SEED_BASE + 32)
+    templates = [rng.standard_normal((SEARCH_L, SEARCH_L)) for _ in range(SEARCH_T)]
+    return spec, templates
+
+
+def _search_peaks(spec, templates, a, b):
+    import numpy as np
+
+    from oracle import fastfft_oracle as O
+
+    fin, fout, iout = (SEARCH_L, SEARCH_L, 1), (SEARCH_N, SEARCH_N, 1), (SEARCH_W, SEARCH_W, 1)
+    plan = O.Plan(fin, fout, fout, iout)
+    vals, idxs = [], []
+    for t in templates[a:b]:
+        win = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), spec, plan, out_dtype=np.float64), iout)
+        i, top, _ = O.peak(win)
+        vals.append(top)
+        idxs.append(i)
+    return torch.tensor(vals, dtype=torch.float64), torch.tensor(idxs, dtype=torch.int64)
+
+
+def _search_worker(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        spec, templates = _search_inputs()          # replicated inputs, prepared locally
+        a, b = shard_range(SEARCH_T, world, rank)
+        v, i = _search_peaks(spec, templates, a, b)
+        gv, gi = gather_peaks(v, i, SEARCH_T)
+        q.put((rank, (a, b), gv.tolist(), gi.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_search_equals_single_rank():
+    spec, templates = _search_inputs()
+    ref_v, ref_i = _search_peaks(spec, templates, 0, SEARCH_T)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_search_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    spans = sorted(r[1] for r in res)
+    assert spans == [(0, 4), (4, 7)]
+    for _, _, v, i in res:
+        assert v == ref_v.tolist()
+        assert i == ref_i.tolist()
