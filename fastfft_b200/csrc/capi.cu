@@ -415,6 +415,7 @@ fastfft_status stage_cols(fastfft_plan_s* h, int n, StageMode mode, int dtype, C
     cudaError_t e = twiddles_for(n, &tw);
     if (e != cudaSuccess) return cuda_fail(h, e, "twiddle table");
     c.tw = tw;
+    c.err = h->dev_err;
     if (mode == ST_FWD)
         e = launch_cols_fwd(n, dtype, c, h->stream);
     else if (mode == ST_INV)

@@ -168,11 +168,13 @@ __device__ __forceinline__ float2 dif_input(float2 x0, float2 x1, float2 x2, int
 // Final radix-3 pass of the inverse.  v: z_k2[n1] of thread (k2 = g.r, j), n1 = j + T' q.
 // Writes them to region k2 of the next buffer, waits for the FFT's threads, then thread t
 // produces x[n1], x[n1 + P], x[n1 + 2P] for n1 = t + T i and hands each to store(n, value).
+// Output pruning: only the outputs n < keep are formed (every output needs all three
+// sub-FFT values, so the pruning is of this last combination only; keep = 3P forms all).
 // The cross-region reads here must be followed by a sync_fft() before any later write to the
 // buffer (the batched kernel's next template begins with one).
 template <int P, class G, class Store>
 __device__ __forceinline__ void dit_output(float2 (&v)[16], G& g, int j, int t, const float2* __restrict__ tw3,
-                                           Store store) {
+                                           Store store, int keep = 3 * P) {
     using S3 = Fft3Shape<P>;
     float2* buf = g.begin_own();
     {
@@ -181,19 +183,26 @@ __device__ __forceinline__ void dit_output(float2 (&v)[16], G& g, int j, int t, 
         for (int q = 0; q < 16; q++) s[phys(j + S3::TP * q)] = v[q];
     }
     g.sync_fft();
+    const int lim = keep < P ? keep : P;
 #pragma unroll 2
     for (int i = 0; i < S3::ROUNDS; i++) {
         const int n1 = t + S3::T * i;
-        if (n1 < P) {
+        if (n1 < lim) {
             const int p = phys(n1);
-            float2 a = buf[p];
+            const float2 a = buf[p];
             const float2 w1 = ld_tw(tw3 + n1), w2 = cmul(w1, w1);  // one load: W^2n1 = (W^n1)^2
-            float2 b = cmulc(buf[G::SUB + p], w1);
-            float2 c = cmulc(buf[2 * G::SUB + p], w2);
-            idft3(a, b, c);
-            store(n1, a);
-            store(n1 + P, b);
-            store(n1 + 2 * P, c);
+            const float2 b = cmulc(buf[G::SUB + p], w1);
+            const float2 c = cmulc(buf[2 * G::SUB + p], w2);
+            // inverse DFT3 of (a, b, c), W_3 = exp(+2 pi i / 3), formed only where kept
+            const float2 s = cadd(b, c);
+            store(n1, cadd(a, s));
+            if (n1 + P < keep) {
+                const float2 d = csub(b, c);
+                const float2 m = make_float2(fmaf(-0.5f, s.x, a.x), fmaf(-0.5f, s.y, a.y));
+                const float hx = kH3 * d.x, hy = kH3 * d.y;
+                store(n1 + P, make_float2(m.x - hy, m.y + hx));
+                if (n1 + 2 * P < keep) store(n1 + 2 * P, make_float2(m.x + hy, m.y - hx));
+            }
         }
     }
 }

@@ -272,6 +272,24 @@ __device__ __forceinline__ void dft16_pruned(float2 (&v)[16], int qnz) {
     dft16_outer<INV>(a, v);
 }
 
+// The first four outputs X[0..3] of DFT16 (the rest of v is left undefined): the last pass
+// of an inverse whose retained window ends within the first quarter of every thread's slots
+// (output pruning; e.g. a 4096-point inverse keeping 1024 outputs).  The first stage and the
+// twiddles are needed by every output; the last stage keeps only its k2 = 0 sums.
+template <bool INV>
+__device__ __forceinline__ void dft16_head4(float2 (&v)[16]) {
+    float2 a[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) a[i] = v[i];
+    dft4<INV>(a[0], a[4], a[8], a[12]);
+    dft4<INV>(a[1], a[5], a[9], a[13]);
+    dft4<INV>(a[2], a[6], a[10], a[14]);
+    dft4<INV>(a[3], a[7], a[11], a[15]);
+    dft16_inner_twiddles<INV>(a);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) v[k1] = cadd(cadd(a[4 * k1], a[4 * k1 + 2]), cadd(a[4 * k1 + 1], a[4 * k1 + 3]));
+}
+
 // ---------------------------------------------------------------------------
 // Pass structure for one size
 // ---------------------------------------------------------------------------
@@ -414,10 +432,14 @@ struct BlockFft {
 
     // Thread j of the FFT, v holds x[j + T q].  g: this FFT group's exchange buffers and
     // barrier.  tw: the twiddle table for size N.  qnz: number of leading q slots that
-    // may be non-zero on input (16 = no pruning).  Every thread of the group must call
-    // this (and, for groups smaller than a warp, every thread of the block).
+    // may be non-zero on input (16 = no pruning).  qout: number of leading output slots
+    // X[j + T q], q < qout, the caller keeps (16 = all); the last pass computes only those
+    // where the pass structure allows it (the others are left undefined).  Every thread of
+    // the group must call this (and, for groups smaller than a warp, every thread of the
+    // block).
     template <class G>
-    __device__ __forceinline__ static void run(float2 (&v)[16], G& g, int j, const float2* __restrict__ tw, int qnz) {
+    __device__ __forceinline__ static void run(float2 (&v)[16], G& g, int j, const float2* __restrict__ tw, int qnz,
+                                               int qout = 16) {
 #pragma unroll
         for (int p = 0; p < S::NP16; p++) {
             const int ns = 1 << (4 * p);
@@ -427,6 +449,8 @@ struct BlockFft {
             }
             if (p == 0)
                 dft16_pruned<INV>(v, qnz);
+            else if (S::REM == 1 && p == S::NP16 - 1 && qout <= 4)
+                dft16_head4<INV>(v);
             else
                 dft16<INV>(v);
             if (p < S::NP16 - 1 || S::REM > 1) {
@@ -458,7 +482,20 @@ struct BlockFft {
                     v[m + r * M] = INV ? cmulc(x, wj[r]) : cmul(x, wj[r]);
                 }
             }
-            radix_pass<R, M>(v);
+            if (qout <= M)
+                radix_head<R, M>(v);  // only the r = 0 outputs X[j + T m] are kept
+            else
+                radix_pass<R, M>(v);
+        }
+    }
+
+    // The r = 0 outputs of the closing pass: v[m] = sum over r of v[m + r M]
+    template <int R, int M>
+    __device__ __forceinline__ static void radix_head(float2 (&v)[16]) {
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+#pragma unroll
+            for (int r = 1; r < R; r++) v[m] = cadd(v[m], v[m + r * M]);
         }
     }
 

@@ -70,6 +70,26 @@ template <> __device__ __forceinline__ float2 ld_cplx_stream<__nv_bfloat162>(con
     return __bfloat1622float2(h);
 }
 
+// Shared-memory loads of the staged image column, kept at their point of use (a plain
+// load could be hoisted above the forward transform, holding 16 more complex values live
+// across it and pushing the kernel past its register budget).
+template <class T> __device__ __forceinline__ float2 lds_cplx(const T* p);
+template <> __device__ __forceinline__ float2 lds_cplx<float2>(const float2* p) {
+    float2 r;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(r.x), "=f"(r.y) : "r"(smem_addr(p)));
+    return r;
+}
+template <> __device__ __forceinline__ float2 lds_cplx<__half2>(const __half2* p) {
+    unsigned int u;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(u) : "r"(smem_addr(p)));
+    return __half22float2(*reinterpret_cast<__half2*>(&u));
+}
+template <> __device__ __forceinline__ float2 lds_cplx<__nv_bfloat162>(const __nv_bfloat162* p) {
+    unsigned int u;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(u) : "r"(smem_addr(p)));
+    return __bfloat1622float2(*reinterpret_cast<__nv_bfloat162*>(&u));
+}
+
 // number of leading q slots (x[j + T q]) that can be non-zero when only n < L is loaded
 template <int T>
 __device__ __forceinline__ int leading_slots(int L, int j) {
@@ -218,6 +238,22 @@ struct ColArgs {
     long long out_stride2;
     long long out_elem_stride;
     int W0;
+    // XCORR with one column per block: the image column is staged in shared memory by a bulk
+    // copy issued at the start of the block, so its load overlaps the forward transform
+    // (set by the launcher when the column is 16-byte aligned; err receives a timeout).
+    int stage_img;
+    int* err;
+};
+
+// Shared-memory plan of cols_kernel (bytes): the FFT groups' exchange buffers, then (when the
+// image column is staged) the column and its barrier.
+template <int N, class ImgC, int FPB>
+struct ColSmem {
+    static constexpr int kXchBytes = FftGroup<N, FPB, true>::BYTES;
+    static constexpr int kImgOff = (kXchBytes + 127) & ~127;
+    static constexpr int kImgBytes = N * (int)sizeof(ImgC);
+    static constexpr int kBarOff = (kImgOff + kImgBytes + 15) & ~15;
+    static constexpr int kStagedBytes = kBarOff + 16;
 };
 
 template <int N, int MODE, class InC, class ImgC, class OutC, int FPB>
@@ -225,14 +261,33 @@ __global__ void __launch_bounds__(FftShape<N>::T * FPB, (FftShape<N>::T * FPB <=
 cols_kernel(ColArgs a) {
     using S = FftShape<N>;
     constexpr int T = S::T;
-    extern __shared__ float2 smem[];
+    extern __shared__ __align__(128) float2 smem[];
     using G = FftGroup<N, FPB, true>;
+    using CS = ColSmem<N, ImgC, FPB>;
     const int f = threadIdx.x / T;
     const int j = threadIdx.x - f * T;
     G g(smem, f);
     const int col = blockIdx.x * FPB + f;
     const bool valid = col < a.n_cols;
     const long long bz = blockIdx.y;
+    // image staging (XCORR, one column per block, block-uniform): thread 0 starts the bulk copy
+    // now; the block waits for it (bounded) just before the conj-multiply
+    unsigned char* const sm_raw = reinterpret_cast<unsigned char*>(smem);
+    const ImgC* img_s = reinterpret_cast<const ImgC*>(sm_raw + CS::kImgOff);
+    uint64_t* img_bar = reinterpret_cast<uint64_t*>(sm_raw + CS::kBarOff);
+    __shared__ int img_ok;
+    bool staged = false;
+    if constexpr (MODE == COL_XCORR && FPB == 1) {
+        staged = a.stage_img && a.intra_kind != 0 && valid;
+        if (staged && threadIdx.x == 0) {
+            mbar_init(img_bar, 1);
+            fence_barrier_init();
+            mbar_arrive_expect_tx(img_bar, (uint32_t)CS::kImgBytes);
+            bulk_g2s(sm_raw + CS::kImgOff,
+                     static_cast<const ImgC*>(a.img) + bz * a.img_batch_stride + (long long)col * a.img_stride,
+                     (uint32_t)CS::kImgBytes, img_bar);
+        }
+    }
     const int in_div = a.in_div > 0 ? a.in_div : 1;
     const InC* pin = static_cast<const InC*>(a.in) + bz * a.in_batch_stride + (long long)(col / in_div) * a.in_stride +
                      (long long)(col % in_div) * a.in_stride2;
@@ -245,13 +300,37 @@ cols_kernel(ColArgs a) {
         v[q] = (a.in_scale != 1.f) ? cscale(x, a.in_scale) : x;
     }
     const int qnz = valid ? leading_slots<T>(a.L, j) : 0;
+    // output pruning: a window at the origin keeps X[j + T q] for q < qout only
+    const int qout = a.W0 == 0 ? leading_slots<T>(a.W, j) : 16;
     if constexpr (MODE == COL_INV) {
-        BlockFft<N, true>::run(v, g, j, a.tw, qnz);
+        BlockFft<N, true>::run(v, g, j, a.tw, qnz, qout);
     } else {
-        BlockFft<N, false>::run(v, g, j, a.tw, qnz);
+        // a forward size decrease keeps the first W outputs too; the correlation's forward
+        // feeds every output to the product
+        BlockFft<N, false>::run(v, g, j, a.tw, qnz, MODE == COL_FWD ? qout : 16);
     }
     if constexpr (MODE == COL_XCORR) {
-        if (a.intra_kind != 0) {
+        if (staged) {
+            // block-uniform: thread 0 waits with the bounds and tells the block; a block whose
+            // copy did not land records the timeout and leaves after one more bounded wait
+            if (threadIdx.x == 0) {
+                const bool ok = mbar_wait(img_bar, 0);
+                img_ok = ok ? 1 : 0;
+                if (!ok) {
+                    if (a.err) atomicExch(a.err, kErrTimeout);
+                    mbar_wait(img_bar, 0);
+                }
+            }
+            __syncthreads();
+            if (!img_ok) return;
+            mbar_wait(img_bar, 0);
+            const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const float2 p = conj_mul(v[q], lds_cplx<ImgC>(img_s + j + T * q));
+                v[q] = (sc != 1.f) ? cscale(p, sc) : p;
+            }
+        } else if (a.intra_kind != 0) {
             const ImgC* pimg = static_cast<const ImgC*>(a.img) + bz * a.img_batch_stride + (long long)col * a.img_stride;
             const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
 #pragma unroll
@@ -262,7 +341,7 @@ cols_kernel(ColArgs a) {
                 v[q] = (sc != 1.f) ? cscale(p, sc) : p;
             }
         }
-        BlockFft<N, true>::run(v, g, j, a.tw, 16);
+        BlockFft<N, true>::run(v, g, j, a.tw, 16, qout);
     }
     if (valid) {
         const int out_div = a.out_div > 0 ? a.out_div : 1;
@@ -379,7 +458,8 @@ c2r_rows_kernel(RowInvArgs a) {
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
-    BlockFft<N, true>::run(v, g, j, a.tw, 16);
+    // output pruning: a window at the origin keeps X[j + T q] for q < qout only
+    BlockFft<N, true>::run(v, g, j, a.tw, 16, a.X0 == 0 ? leading_slots<T>(a.W, j) : 16);
     const int ra = 2 * (blockIdx.x * FPB + f);
     OutT* oa = static_cast<OutT*>(a.out[gb]) + (long long)ra * a.out_pitch;
     OutT* ob = oa + a.out_pitch;

@@ -200,7 +200,7 @@ c2r3_rows_kernel(RowInvArgs a) {
                 if (has_a) st_real<OutT>(oa + n, x.x * a.scale);
                 if (has_b) st_real<OutT>(ob + n, x.y * a.scale);
             }
-        });
+        }, a.W);
         return;
     } else {
         const bool write = !a.peaks_only;
@@ -230,7 +230,7 @@ c2r3_rows_kernel(RowInvArgs a) {
                     }
                 }
             }
-        });
+        }, a.X0 + a.W);
         if (a.peaks) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -321,7 +321,7 @@ cols3_kernel(ColArgs a) {
     dit_output<P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
         const int n = n0 - a.W0;
         if (n >= 0 && n < W) pout[n] = (a.out_scale != 1.f) ? cscale(x, a.out_scale) : x;
-    });
+    }, a.W0 + W);
 }
 
 // ---------------------------------------------------------------------------
@@ -450,7 +450,7 @@ xcorr3_cols_kernel(XcorrColArgs a) {
         const int W = live ? a.W : 0;
         dit_output<P>(v, grp, j, t, a.tw3, [&](int n, float2 x) {
             if (n < W) o[n] = x;
-        });
+        }, a.W);
     }
 }
 

@@ -20,26 +20,6 @@
 
 namespace ffb {
 
-// Shared-memory loads of the staged image column, kept at their point of use (a plain
-// load could be hoisted above the forward transform, holding 16 more complex values live
-// across it and pushing the kernel past its register budget).
-template <class T> __device__ __forceinline__ float2 lds_cplx(const T* p);
-template <> __device__ __forceinline__ float2 lds_cplx<float2>(const float2* p) {
-    float2 r;
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(r.x), "=f"(r.y) : "r"(smem_addr(p)));
-    return r;
-}
-template <> __device__ __forceinline__ float2 lds_cplx<__half2>(const __half2* p) {
-    unsigned int u;
-    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(u) : "r"(smem_addr(p)));
-    return __half22float2(*reinterpret_cast<__half2*>(&u));
-}
-template <> __device__ __forceinline__ float2 lds_cplx<__nv_bfloat162>(const __nv_bfloat162* p) {
-    unsigned int u;
-    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(u) : "r"(smem_addr(p)));
-    return __bfloat1622float2(*reinterpret_cast<__nv_bfloat162*>(&u));
-}
-
 struct XcorrColArgs {
     const float2* t1;          // template g, column c: t1 + g * t1_batch + c * t1_pitch (L valid values)
     long long t1_pitch;
@@ -153,7 +133,8 @@ xcorr_cols_kernel(XcorrColArgs a) {
                 for (int q = 0; q < 16; q++) v[q] = cscale(conj_mul(v[q], lds_cplx<ImgC>(img_s + j + T * q)), sc);
             }
         }
-        BlockFft<N, true>::run(v, grp, j, a.tw, 16);
+        // output pruning: only X[j + T q] < W are kept
+        BlockFft<N, true>::run(v, grp, j, a.tw, 16, leading_slots<T>(a.W, j));
         if (live) {
             float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
 #pragma unroll

@@ -4,13 +4,22 @@
 namespace ffb {
 
 template <int N, int MODE, class ImgC, class InC = float2, class OutC = float2>
-static cudaError_t cols_impl(const ColArgs& a, cudaStream_t st) {
+static cudaError_t cols_impl(const ColArgs& args, cudaStream_t st) {
     constexpr int FPB = col_fpb<N>();
     constexpr int THREADS = FftShape<N>::T * FPB;
-    const size_t smem = (size_t)FftGroup<N, FPB, true>::BYTES;
-    static std::atomic<unsigned long long> mask{0};
+    using CS = ColSmem<N, ImgC, FPB>;
+    ColArgs a = args;
+    // The fused pass with one column per block stages its image column by a bulk copy when
+    // every column starts on a 16-byte boundary (cp.async.bulk needs 16-byte aligned
+    // addresses and sizes; N * sizeof(ImgC) is a multiple of 16 for N >= 16).
+    const size_t isz = sizeof(ImgC);
+    a.stage_img = MODE == COL_XCORR && FPB == 1 && a.intra_kind != 0 && a.img != nullptr &&
+                  reinterpret_cast<uintptr_t>(a.img) % 16 == 0 && (a.img_stride * isz) % 16 == 0 &&
+                  (a.img_batch_stride * isz) % 16 == 0;
+    const size_t smem = a.stage_img ? (size_t)CS::kStagedBytes : (size_t)CS::kXchBytes;
+    static std::atomic<int> high_water[64];
     auto fn = cols_kernel<N, MODE, InC, ImgC, OutC, FPB>;
-    cudaError_t e = ensure_smem_attr((const void*)fn, smem, &mask);
+    cudaError_t e = ensure_smem_at_least((const void*)fn, smem, high_water);
     if (e != cudaSuccess) return e;
     const int grid = (a.n_cols + FPB - 1) / FPB;
     if (grid == 0) return cudaSuccess;
