@@ -674,13 +674,48 @@ def run_cufft(dev, images, templates, window0, corr, batch_full=16):
     win = reduced_step()[0].cpu().numpy()
     ours = window0.reshape(W, -1)[:, :W]
     rel = float(np.linalg.norm(win - ours) / np.linalg.norm(ours))
-    return {"full_size": {"value": batch_full / (ms_full * 1e-3), "unit": UNIT,
+    recipe = run_cufft_recipe(tv[0].cpu().numpy(), specs_c[0].contiguous().cpu().numpy(), ours)
+    return {"callback_recipe": recipe,
+            "full_size": {"value": batch_full / (ms_full * 1e-3), "unit": UNIT,
                           "how": f"torch.fft (cuFFT), batches of {batch_full}: pad to 4096^2, rfft2, conj-multiply, "
                                  "irfft2, crop to 1024^2"},
             "reduced_size": {"value": B / (ms_red * 1e-3), "unit": UNIT, "correlation_size": [mx, my],
                              "how": f"torch.fft (cuFFT), {B} templates per step: image crop spectrum (irfft2 4096^2, "
                                     f"crop, rfft2 at {mx}x{my}) then pad, rfft2, conj-multiply, irfft2, crop",
                              "rel_l2_vs_ours": rel}}
+
+
+def run_cufft_recipe(template, image_kykx, ours):
+    """The reference's own cuFFT recipe (clip into the top-left of a zeroed 4096^2 buffer,
+    in-place R2C, in-place C2R with a conj-multiply load callback, full 4096^2 output) as a
+    separate program (fastfft_b200/bin/cufft_recipe_bench, its own process so that it uses the
+    toolkit's cuFFT and nvJitLink), one template per execution as in the reference and 16 per
+    execution; the window of its output is compared with ours."""
+    import tempfile
+
+    exe = os.path.join(ROOT, "fastfft_b200", "bin", "cufft_recipe_bench")
+    fatbin = os.path.join(ROOT, "fastfft_b200", "bin", "cufft_recipe_cb.fatbin")
+    if not (os.path.exists(exe) and os.path.exists(fatbin)):
+        return {"unavailable": "comparator program not built (python -m fastfft_b200.build)"}
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        np.ascontiguousarray(template, dtype=np.float32).tofile(os.path.join(d, "template.f32"))
+        np.ascontiguousarray(image_kykx, dtype=np.complex64).tofile(os.path.join(d, "image_kykx.c64"))
+        for batch, reps in ((1, 40), (16, 6)):
+            p = subprocess.run([exe, d, str(N), str(L), str(batch), str(reps), fatbin, str(W)], capture_output=True,
+                               text=True, timeout=300)
+            try:
+                r = json.loads(p.stdout.strip().splitlines()[-1])
+            except (ValueError, IndexError):
+                r = {"error": (p.stdout + p.stderr)[-300:]}
+            if "ms_per_execution" in r:
+                win = np.fromfile(os.path.join(d, "corr.f32"), dtype=np.float32).reshape(W, N + 2)[:, :W]
+                r = {"value": batch / (r["ms_per_execution"] * 1e-3), "unit": UNIT,
+                     "rel_l2_vs_ours": float(np.linalg.norm(win - ours) / np.linalg.norm(ours))}
+            out[f"templates_per_execution_{batch}"] = r
+    out["how"] = ("cuFFT 4096^2: clip into top-left, in-place R2C, in-place C2R with an LTO load callback "
+                  "conj(T) x I (the reference's padded_convolution_FastFFT_vs_cuFFT recipe), full output")
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -937,7 +972,9 @@ def run_ours(args, world, rank, local):
     cufft = None
     if rank == 0 and not args.skip_cufft:
         cufft = run_cufft(dev, images, templates, window0, corr_now)
-        strongest = max(cufft["full_size"]["value"], cufft["reduced_size"]["value"])
+        cands = [cufft["full_size"]["value"], cufft["reduced_size"]["value"]]
+        cands += [v["value"] for k, v in cufft["callback_recipe"].items() if isinstance(v, dict) and "value" in v]
+        strongest = max(cands)
         cufft["ours_over_strongest"] = value / world / strongest
 
     # ---- the other workload families (rank 0) ----

@@ -85,12 +85,21 @@ size_t real_size(int d) { return d == FASTFFT_DTYPE_F32 ? 4 : 2; }
 
 long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 
-// ReturnPaddedMemorySize (include/FastFFT.h:363-404) for real-valued InputType.
-long long padded_elems(Dims& d) {
+// ReturnPaddedMemorySize (include/FastFFT.h:363-404): real InputType rows hold w = x/2 + 1
+// complex values after the R2C (FFTW pitch 2w); complex InputType rows hold w = x.  The
+// count is in scalar components (two per complex value).
+long long padded_elems(Dims& d, bool complex_input = false) {
+    if (complex_input) {
+        d.w = d.x;
+        return 2LL * d.x * d.y * d.z;
+    }
     const int jump = (d.x % 2 == 0) ? 2 : 1;
     d.w = (d.x + jump) / 2;
     return 2LL * d.w * d.y * d.z;
 }
+
+// Spectrum columns kx of a length-n x axis: n/2 + 1 for real input, n for complex input.
+long long kx_count(const fastfft_plan_s* h, long long n) { return cplx_dtype(h->input_dtype) ? n : n / 2 + 1; }
 
 // Classify one direction (FastFFT.cu:803-850).  Mixed growth/shrink is rejected.
 bool classify(const Dims& in, const Dims& out, SizeChange* sc, std::string* why) {
@@ -129,10 +138,11 @@ fastfft_status validate(fastfft_plan_s* h) {
                 return fail(h, FASTFFT_ERR_INVALID_DIMS, "all dimensions must be <= 512 for 3d transforms");
     }
     if (dim != h->rank) return fail(h, FASTFFT_ERR_INVALID_DIMS, "plan dimensionality does not match the handle rank");
-    // transform lengths: powers of two (FastFFT.cu:895-927); 2D plans also take 3 * 2^k with
-    // 128 <= 2^k <= 2048 (384 ... 6144), which the reference rejects
-    auto len_ok = [&](long long v) { return is_pow2(v) || (dim == 2 && v <= 6144 && ffb::is_3p_size((int)v)); };
-    const char* lens = dim == 2 ? "powers of 2 or 3 * 2^k (384 ... 6144)" : "powers of 2";
+    // transform lengths: powers of two (FastFFT.cu:895-927); real-input 2D plans also take
+    // 3 * 2^k with 128 <= 2^k <= 2048 (384 ... 6144), which the reference rejects
+    const bool wide = dim == 2 && !cplx_dtype(h->input_dtype);
+    auto len_ok = [&](long long v) { return is_pow2(v) || (wide && v <= 6144 && ffb::is_3p_size((int)v)); };
+    const char* lens = wide ? "powers of 2 or 3 * 2^k (384 ... 6144)" : "powers of 2";
     if ((!len_ok(fi.x) || !len_ok(fi.y) || !is_pow2(fi.z)) && h->fwd_change != SizeChange::Increase)
         return fail(h, FASTFFT_ERR_INVALID_DIMS,
                     std::string("input dimensions must be ") + lens + " unless the forward transform pads");
@@ -177,8 +187,8 @@ long long corr_size_at_least(long long v) {
 void size_buffers(fastfft_plan_s* h) {
     h->prepared_image = nullptr;
     const long long nx_f = std::max(h->fwd_in.x, h->fwd_out.x);
-    const long long kx_f = nx_f / 2 + 1;
-    const long long kx_i = h->inv_in.x / 2 + 1;
+    const long long kx_f = kx_count(h, nx_f);
+    const long long kx_i = kx_count(h, h->inv_in.x);
     if (h->rank == 3) {
         // A: forward [kx][y][z] (pitch round_up(Ly*Lz, 4)) / inverse [kx][y'][kz]
         // B: forward [kz][kx][y] / inverse [kx][z'][y'] (pitch round_up(Wz*Wy, 4))
@@ -201,7 +211,7 @@ void size_buffers(fastfft_plan_s* h) {
     h->red_ok = false;
     h->bytes_c = 0;
     const bool origin0 = h->org_x == 0 && h->org_y == 0 && h->org_z == 0;
-    if (origin0 && h->fwd_change != SizeChange::Decrease && h->inv_change == SizeChange::Decrease) {
+    if (origin0 && !cplx_dtype(h->input_dtype) && h->fwd_change != SizeChange::Decrease && h->inv_change == SizeChange::Decrease) {
         const long long nx = h->fwd_out.x, ny = h->fwd_out.y;
         const long long mx = std::min(nx, corr_size_at_least(h->fwd_in.x + h->inv_out.x - 1));
         const long long my = std::min(ny, corr_size_at_least(h->fwd_in.y + h->inv_out.y - 1));
@@ -351,8 +361,13 @@ fastfft_status stage_r2c(fastfft_plan_s* h, int n, int in_dtype, const void* in,
     a.kmax = kmax;
     a.scale = scale;
     a.tw = tw;
-    e = launch_r2c_rows(n, in_dtype, a, h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "r2c row pass");
+    if (cplx_dtype(in_dtype)) {
+        a.in_pitch = in_pitch / 2;  // pitches arrive in scalar components; complex rows hold half as many
+        e = launch_c2c_rows_fwd(n, in_dtype, a, h->stream);
+    } else {
+        e = launch_r2c_rows(n, in_dtype, a, h->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(h, e, "row pass (forward)");
     h->launches++;
     prof_mark(h);
     return FASTFFT_OK;
@@ -381,8 +396,14 @@ fastfft_status stage_c2r(fastfft_plan_s* h, int n, const float2* in, long long i
     a.peak_slot[0] = peak_slot;
     a.mip = mip;
     a.mip_base = mip_base;
-    e = launch_c2r_rows(n, h->output_dtype, a, h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "c2r row pass");
+    if (cplx_dtype(h->output_dtype)) {
+        if (peaks || mip) return fail(h, FASTFFT_ERR_UNSUPPORTED, "peak search and projection need real output");
+        a.out_pitch = out_pitch / 2;  // pitches arrive in scalar components
+        e = launch_c2c_rows_inv(n, h->output_dtype, a, h->stream);
+    } else {
+        e = launch_c2r_rows(n, h->output_dtype, a, h->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(h, e, "row pass (inverse)");
     h->launches++;
     prof_mark(h);
     return FASTFFT_OK;
@@ -468,7 +489,7 @@ fastfft_status seq_fwd(fastfft_plan_s* h, const void* in, void* out, float pre_s
 fastfft_status seq_inv(fastfft_plan_s* h, const void* in, int in_dtype, void* out, float post_scale) {
     const Dims &ii = h->inv_in, &io = h->inv_out;
     const int nx = (int)ii.x, ny = (int)ii.y, nz = (int)ii.z;
-    const int kw = nx / 2 + 1;
+    const int kw = (int)kx_count(h, nx);
     if (h->rank == 2) {
         ColArgs c = col_args(in, ny, ny, region_b(h), h->pitch_b, (int)io.y, kw);
         c.W0 = (int)h->org_y;
@@ -505,8 +526,8 @@ fastfft_status seq_xcorr_sized(fastfft_plan_s* h, const void* in, int lx, int ly
                                unsigned long long* mip = nullptr, int mip_base = 0) {
     const Dims &fo = h->fwd_out, &io = h->inv_out;
     const int nx = (int)fo.x, ny = (int)fo.y;
-    const int kw = nx / 2 + 1;
-    const long long pitch = 2LL * ((lx + (lx % 2 == 0 ? 2 : 1)) / 2);
+    const int kw = (int)kx_count(h, nx);
+    const long long pitch = cplx_dtype(h->input_dtype) ? 2LL * lx : 2LL * ((lx + (lx % 2 == 0 ? 2 : 1)) / 2);
     FFB_TRY(stage_r2c(h, nx, h->input_dtype, in, pitch, ly, ly, 1, lx, region_a(h), h->pitch_a, kw, pre_scale));
     ColArgs c = col_args(region_a(h), h->pitch_a, ly, region_b(h), h->pitch_b, (int)io.y, kw);
     c.img = img;
@@ -524,7 +545,7 @@ fastfft_status seq_xcorr(fastfft_plan_s* h, const void* in, const void* img, voi
                          const fastfft_op* intra_op, float post_scale) {
     const Dims &fi = h->fwd_in, &fo = h->fwd_out, &io = h->inv_out;
     const int nx = (int)fo.x, ny = (int)fo.y, nz = (int)fo.z;
-    const int kw = nx / 2 + 1;
+    const int kw = (int)kx_count(h, nx);
     const int ikind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
     const float iscale = intra_op ? intra_op->scale : 1.f;
     if (h->rank == 2) {
@@ -586,7 +607,8 @@ fastfft_status fastfft_create(fastfft_handle* out, int compute_dtype, int input_
     if (!out) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle pointer");
     *out = nullptr;
     if (compute_dtype != FASTFFT_DTYPE_F32) return fail(nullptr, FASTFFT_ERR_UNSUPPORTED, "compute type must be float");
-    if (!real_dtype(input_dtype)) return fail(nullptr, FASTFFT_ERR_UNSUPPORTED, "input type must be a real type (f32, f16, bf16)");
+    if (!real_dtype(input_dtype) && !cplx_dtype(input_dtype))
+        return fail(nullptr, FASTFFT_ERR_UNSUPPORTED, "input type must be f32, f16, bf16, c64, c32h or c32bf");
     if (!cplx_dtype(image_dtype)) return fail(nullptr, FASTFFT_ERR_UNSUPPORTED, "image type must be complex (c64, c32h, c32bf)");
     if (rank != 2 && rank != 3) return fail(nullptr, FASTFFT_ERR_UNSUPPORTED, "only 2D and 3D FFTs are supported");
     fastfft_plan_s* h = new (std::nothrow) fastfft_plan_s();
@@ -635,7 +657,8 @@ static fastfft_status set_plan(fastfft_handle h, bool fwd, size_t ix, size_t iy,
         return fail(h, FASTFFT_ERR_INVALID_DIMS, "logical dimensions must be < 32768");
     if (!is_padded) return fail(h, FASTFFT_ERR_UNSUPPORTED, "input arrays must be FFTW padded");
     Dims in{(long long)ix, (long long)iy, (long long)iz, 0}, outd{(long long)ox, (long long)oy, (long long)oz, 0};
-    const long long n_in = padded_elems(in), n_out = padded_elems(outd);
+    const bool cx = cplx_dtype(h->input_dtype);
+    const long long n_in = padded_elems(in, cx), n_out = padded_elems(outd, cx);
     if (fwd) {
         h->fwd_in = in;
         h->fwd_out = outd;
@@ -801,7 +824,10 @@ fastfft_status fastfft_set_inverse_output_origin(fastfft_handle h, size_t ox, si
 
 fastfft_status fastfft_set_output_dtype(fastfft_handle h, int dtype) {
     if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
-    if (!real_dtype(dtype)) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "output dtype must be real (f32, f16, bf16)");
+    if (cplx_dtype(h->input_dtype) ? !cplx_dtype(dtype) : !real_dtype(dtype))
+        return fail(h, FASTFFT_ERR_INVALID_ARGUMENT,
+                    cplx_dtype(h->input_dtype) ? "output dtype of a complex-input plan must be complex (c64, c32h, c32bf)"
+                                               : "output dtype must be real (f32, f16, bf16)");
     h->output_dtype = dtype;
     return FASTFFT_OK;
 }

@@ -18,6 +18,9 @@ struct XcorrColArgs;
 // dtype codes follow fastfft_dtype in include/fastfft_capi.h
 cudaError_t launch_r2c_rows(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
 cudaError_t launch_c2r_rows(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
+// Complex-input row passes (in_dtype / out_dtype: 3 complex64, 4 complex32, 5 complex bf16).
+cudaError_t launch_c2c_rows_fwd(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
+cudaError_t launch_c2c_rows_inv(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
 // out_dtype: storage of the spectrum written (3 complex64, 4 complex32, 5 complex bf16)
 cudaError_t launch_cols_fwd(int n, int out_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_cols_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st);

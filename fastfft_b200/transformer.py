@@ -19,6 +19,9 @@ from . import _capi as C
 _REAL_DTYPES = {"float32": C.DTYPE_F32, "float16": C.DTYPE_F16, "bfloat16": C.DTYPE_BF16}
 _CPLX_DTYPES = {"complex64": C.DTYPE_C64, "complex32": C.DTYPE_C32H, "chalf": C.DTYPE_C32H,
                 "complex_bf16": C.DTYPE_C32BF}
+# InputType: real (R2C / C2R transforms) or complex (C2C transforms; the reference declares
+# complex InputType but leaves its paths as stubs, src/fastfft/FastFFT.cu:369-391)
+_INPUT_DTYPES = {**_REAL_DTYPES, **_CPLX_DTYPES}
 
 
 def _dtype_code(name, table):
@@ -80,12 +83,13 @@ class FourierTransformer:
         self._lib = C.lib()
         self._h = C.Handle()
         st = self._lib.fastfft_create(ctypes.byref(self._h), _dtype_code(compute_dtype, {"float32": 0}),
-                                      _dtype_code(input_dtype, _REAL_DTYPES),
+                                      _dtype_code(input_dtype, _INPUT_DTYPES),
                                       _dtype_code(image_dtype, _CPLX_DTYPES), int(rank))
         if st != C.OK:
             raise C.FastFFTError(st, self._lib.fastfft_last_error(None).decode())
         self._stream = None
         self.rank = rank
+        self.complex_input = str(input_dtype).replace("torch.", "") in _CPLX_DTYPES
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -130,7 +134,9 @@ class FourierTransformer:
         self._check(self._lib.fastfft_set_inverse_output_origin(self._h, ox, oy, oz))
 
     def SetOutputDtype(self, dtype):
-        self._check(self._lib.fastfft_set_output_dtype(self._h, _dtype_code(dtype, _REAL_DTYPES)))
+        """Storage of the inverse's output: real for real-input plans, complex for complex-input plans."""
+        table = _CPLX_DTYPES if self.complex_input else _REAL_DTYPES
+        self._check(self._lib.fastfft_set_output_dtype(self._h, _dtype_code(dtype, table)))
 
     # -- transforms ------------------------------------------------------
     def FwdFFT(self, input_ptr, output_ptr=None, pre_op=None, intra_op=None):

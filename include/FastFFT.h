@@ -10,6 +10,8 @@
 //
 // Differences a caller can see:
 //   - InputType may also be __nv_bfloat16 and OtherImageType __nv_bfloat162;
+//   - complex InputType (float2, __half2, __nv_bfloat162) runs C2C transforms (the reference
+//     declares it but stubs its paths, FastFFT.cu:369-391);
 //   - the cross-correlation with a forward increase and an inverse decrease (the
 //     reference's "work in progress" abort, FastFFT.cu:673-679) is implemented;
 //   - work goes to cudaStreamPerThread unless SetStream() is called.
@@ -102,13 +104,16 @@ template <class ComputeBaseType = float, class InputType = float, class OtherIma
 class FourierTransformer {
     static_assert(std::is_same_v<ComputeBaseType, float>, "Compute base type must be float");
     static_assert(Rank == 2 || Rank == 3, "Only 2D and 3D FFTs are supported");
-    static_assert(detail::real_dtype<InputType>() >= 0, "Input type must be float, __half or __nv_bfloat16");
+    static_assert(detail::real_dtype<InputType>() >= 0 || detail::complex_dtype<InputType>() >= 0,
+                  "Input type must be float, __half, __nv_bfloat16, float2, __half2 or __nv_bfloat162");
     static_assert(detail::complex_dtype<OtherImageType>() >= 0,
                   "OtherImageType must be float2, __half2 or __nv_bfloat162");
 
   public:
     FourierTransformer() {
-        check(fastfft_create(&h_, FASTFFT_DTYPE_F32, detail::real_dtype<InputType>(),
+        check(fastfft_create(&h_, FASTFFT_DTYPE_F32,
+                             detail::real_dtype<InputType>() >= 0 ? detail::real_dtype<InputType>()
+                                                                  : detail::complex_dtype<InputType>(),
                              detail::complex_dtype<OtherImageType>(), Rank),
               "FourierTransformer");
     }

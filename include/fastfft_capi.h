@@ -71,8 +71,10 @@ typedef struct {
 } fastfft_op;
 
 /* FourierTransformer() constructor (FastFFT.cu:58-74).  compute_dtype must be F32;
- * input_dtype F32/F16/BF16 (real data; the reference's InputType); image_dtype
- * C64/C32H/C32BF (OtherImageType); rank 2 or 3. */
+ * input_dtype F32/F16/BF16 (real data, R2C / C2R transforms) or C64/C32H/C32BF (complex
+ * data, C2C transforms: the reference's complex InputType, whose paths it leaves as stubs,
+ * FastFFT.cu:369-391; spectra keep the [kx][ky] layout with kx over all N_x, rows have
+ * pitch x, powers of two only); image_dtype C64/C32H/C32BF (OtherImageType); rank 2 or 3. */
 FASTFFT_API fastfft_status fastfft_create(fastfft_handle* out, int compute_dtype, int input_dtype, int image_dtype,
                               int rank);
 /* ~FourierTransformer() (FastFFT.cu:76-80, Deallocate :105-113). */
@@ -95,7 +97,8 @@ FASTFFT_API fastfft_status fastfft_set_stream(fastfft_handle h, void* cuda_strea
  * batched correlation's reduced-size path needs the origin at 0 and falls back to the
  * size-N kernels otherwise.  No reference counterpart. */
 FASTFFT_API fastfft_status fastfft_set_inverse_output_origin(fastfft_handle h, size_t ox, size_t oy, size_t oz);
-/* Real output dtype of InvFFT / FwdImageInvFFT (default: input_dtype, as in the reference). */
+/* Output dtype of InvFFT / FwdImageInvFFT (default: input_dtype, as in the reference): real
+ * for real-input plans, complex for complex-input plans. */
 FASTFFT_API fastfft_status fastfft_set_output_dtype(fastfft_handle h, int dtype);
 /* Storage of the spectrum FwdFFT writes: FASTFFT_DTYPE_C64 (default), C32H or C32BF, each
  * value multiplied by `scale` (1 = as computed) and rounded to nearest once in the last pass:

@@ -248,6 +248,69 @@ def fwd_image_inv(t_padded: np.ndarray, image_spectrum: np.ndarray, plan: Plan,
 
 
 # ---------------------------------------------------------------------------
+# Complex-input (C2C) transforms.  The reference declares complex InputType but leaves its
+# complex paths as stubs (src/fastfft/FastFFT.cu:369-391, 3D cross-correlation :722-793);
+# these follow the conventions of its real path: sign -1 forward, unnormalised, zero padding
+# at the origin, the transposed spectrum layout [kz][kx][ky] (kx now over all N_x), the
+# window of a decrease at the origin (or at `origin`), complex rows of pitch x
+# (ReturnPaddedMemorySize's complex branch, include/FastFFT.h:381-384).
+# ---------------------------------------------------------------------------
+
+def complex_memory_size(dims: tuple[int, int, int]) -> int:
+    """Scalar components the reference reserves for complex dims (x, y, z): 2 x y z."""
+    x, y, z = dims
+    return 2 * x * y * z
+
+
+def complex_from_buffer(buf: np.ndarray, dims: tuple[int, int, int]) -> np.ndarray:
+    """View a flat complex buffer (interleaved re, im; rows of pitch x) as a (z, y, x) array."""
+    x, y, z = dims
+    a = np.asarray(buf).reshape(-1)
+    if not np.iscomplexobj(a):
+        a = a[: 2 * x * y * z].astype(np.float64).view(np.complex128)
+    return a[: x * y * z].reshape(z, y, x)
+
+
+def complex_to_buffer(a: np.ndarray, dtype=np.complex64) -> np.ndarray:
+    """Flat interleaved buffer of a complex (z, y, x) array (rows of pitch x)."""
+    return np.ascontiguousarray(np.asarray(a).reshape(-1).astype(dtype))
+
+
+def fwd_c2c(x: np.ndarray, fwd_in, fwd_out, pre_op=(OP_NOOP, 1.0), dtype=np.complex128) -> np.ndarray:
+    """C2C FwdFFT: complex (z, y, x) input of dims fwd_in -> spectrum [kz][kx][ky] of dims
+    fwd_out (first outputs per axis kept on a decrease), shape (out.z, out.x, out.y)."""
+    fwd_in, fwd_out = tuple(fwd_in), tuple(fwd_out)
+    nx, ny, nz = (max(a, b) for a, b in zip(fwd_in, fwd_out))
+    src = apply_scale(np.asarray(x, dtype=dtype).reshape(fwd_in[2], fwd_in[1], fwd_in[0]), pre_op[0], pre_op[1])
+    full = np.zeros((nz, ny, nx), dtype=dtype)
+    full[: fwd_in[2], : fwd_in[1], : fwd_in[0]] = src
+    s = np.fft.fftn(full, axes=(0, 1, 2) if nz > 1 else (1, 2))
+    s = s[: fwd_out[2], : fwd_out[1], : fwd_out[0]]
+    return spectrum_from_zyx(s)
+
+
+def inv_c2c(s_ref: np.ndarray, inv_in, inv_out, post_op=(OP_NOOP, 1.0), origin=(0, 0, 0)) -> np.ndarray:
+    """C2C InvFFT: spectrum [kz][kx][ky] of dims inv_in -> complex (z, y, x) window of dims
+    inv_out at `origin`, unnormalised (a round trip scales by Nx Ny Nz)."""
+    nx, ny, nz = tuple(inv_in)
+    s = np.asarray(s_ref, dtype=np.complex128).reshape(nz, nx, ny)
+    r = np.fft.ifftn(spectrum_to_zyx(s), axes=(0, 1, 2) if nz > 1 else (1, 2)) * (nx * ny * nz)
+    ox, oy, oz = origin
+    r = r[oz: oz + inv_out[2], oy: oy + inv_out[1], ox: ox + inv_out[0]]
+    return apply_scale(r, post_op[0], post_op[1])
+
+
+def fwd_image_inv_c2c(t: np.ndarray, image_spectrum: np.ndarray, plan: Plan, pre_op=(OP_NOOP, 1.0),
+                      intra_op=(OP_CONJ_MUL, 1.0), post_op=(OP_NOOP, 1.0), origin=(0, 0, 0)) -> np.ndarray:
+    """C2C FwdImageInvFFT: conj(fft(T_pad)) x image spectrum (full [kz][kx][ky] layout), inverse,
+    window.  c[r] = N sum_x conj(T(x)) I(x + r) (mod N)."""
+    t_hat = fwd_c2c(t, plan.fwd_in, plan.fwd_out, pre_op)
+    img = np.asarray(image_spectrum).reshape(t_hat.shape)
+    prod = apply_intra(t_hat, img.astype(np.complex128), intra_op[0], intra_op[1])
+    return inv_c2c(prod, plan.inv_in, plan.inv_out, post_op, origin=origin)
+
+
+# ---------------------------------------------------------------------------
 # Metrics
 # ---------------------------------------------------------------------------
 

@@ -109,11 +109,10 @@ def test_transform_before_plan_is_an_error():
 
 
 def test_bad_dtypes_and_zero_dims():
-    with pytest.raises(F.FastFFTError):
-        C.lib()  # loads
-        h = C.Handle()
-        st = C.lib().fastfft_create(ctypes.byref(h), 0, C.DTYPE_C64, C.DTYPE_C64, 2)
-        raise F.FastFFTError(st, "real input required") if st != C.OK else AssertionError("accepted complex input")
+    h = C.Handle()
+    assert C.lib().fastfft_create(ctypes.byref(h), 0, 9, C.DTYPE_C64, 2) == C.ERR_UNSUPPORTED      # no such dtype
+    assert C.lib().fastfft_create(ctypes.byref(h), 0, C.DTYPE_F32, C.DTYPE_F32, 2) == C.ERR_UNSUPPORTED  # real image
+    assert C.lib().fastfft_create(ctypes.byref(h), 1, C.DTYPE_F32, C.DTYPE_C64, 2) == C.ERR_UNSUPPORTED  # compute
     ft = new()
     with pytest.raises(F.FastFFTError) as e:
         ft.SetForwardFFTPlan(0, 64, 1, 64, 64, 1)
@@ -155,3 +154,35 @@ def test_radial_operations_validate_arguments():
     ft.SetSpectrumOutput("complex32", 1.0)
     # in place needs complex64 storage
     assert lib.fastfft_apply_radial_filter(ft._h, 0x1000, 0x1000, 64, 0x2000, 10) == C.ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("fin,fout,iout", [
+    ((64, 64, 1), (512, 512, 1), (512, 512, 1)),
+    ((384, 200, 1), (4096, 2048, 1), (1000, 999, 1)),
+    ((64, 64, 64), (256, 256, 256), (128, 128, 128)),
+])
+def test_complex_input_memory_sizes(fin, fout, iout):
+    """Complex InputType: 2 x y z scalar components, w = x (include/FastFFT.h:381-384)."""
+    ft = new(rank=3 if fout[2] > 1 else 2, input_dtype="complex64")
+    ft.SetForwardFFTPlan(*fin, *fout)
+    ft.SetInverseFFTPlan(*fout, *iout)
+    assert ft.ReturnInputMemorySize() == O.complex_memory_size(fin)
+    assert ft.ReturnFwdOutputMemorySize() == O.complex_memory_size(fout)
+    assert ft.ReturnInvOutputMemorySize() == O.complex_memory_size(iout)
+    assert ft.ReturnFwdInputDimensions() == (*fin, fin[0])
+    assert ft.ReturnFwdOutputDimensions() == (*fout, fout[0])
+
+
+def test_complex_input_rules():
+    ft = new(input_dtype="complex64")
+    with pytest.raises(ValueError):
+        ft.SetOutputDtype("float32")            # complex-input plans write complex output
+    assert C.lib().fastfft_set_output_dtype(ft._h, C.DTYPE_F32) == C.ERR_INVALID_ARGUMENT
+    ft.SetOutputDtype("complex_bf16")
+    ft.SetForwardFFTPlan(64, 64, 1, 384, 384, 1)
+    with pytest.raises(C.FastFFTError):           # 3 * 2^k lengths are real-input only
+        ft.SetInverseFFTPlan(384, 384, 1, 384, 384, 1)
+    real = new()
+    with pytest.raises(ValueError):
+        real.SetOutputDtype("complex64")
+    assert C.lib().fastfft_set_output_dtype(real._h, C.DTYPE_C64) == C.ERR_INVALID_ARGUMENT
