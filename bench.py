@@ -94,7 +94,7 @@ def pass_bytes_per_template(corr, t_xy, w_xy, per_launch, n_per_call, t_size=4, 
     return [r2c, cols, c2r, prep]
 
 
-def config(templates_per_step, corr_size=None, per_launch=None):
+def config(templates_per_step, corr_size=None, per_launch=None, groups=None, tuned=None):
     return {
         "workload": "2D fused cross-correlation FP32: 384^2 template zero-padded to 4096^2, conj-multiply with a "
                     "resident 4096^2 image spectrum, inverse cropped to a 1024^2 window",
@@ -102,6 +102,8 @@ def config(templates_per_step, corr_size=None, per_launch=None):
         "templates_per_step": templates_per_step,
         "correlation_size": list(corr_size) if corr_size else None,
         "templates_per_launch": per_launch,
+        "groups_in_flight": groups,
+        "autotune_ms_per_step": tuned,
         "image_spectra": N_IMAGES,
         "l2": "3 image spectra of 67 MB per GPU rotate step by step (201 MB > 126 MB L2): each step reads its "
               "image spectrum from HBM and prepares its cropped correlation-size spectrum inside the timed step",
@@ -368,6 +370,7 @@ def run_uneven(dev, image_f32, storage, local, min_seconds, check=True):
                        "4096^2 image spectrum, 512^2 windows; the whole batch is one CUDA graph launch",
            "storage": storage, "value": UNEVEN_N_TEMPLATES / (ms * 1e-3), "unit": UNIT, "ms_per_batch": ms,
            "timed_batches": reps, "correlation_size": list(ft.CorrelationSize()), "templates_per_launch": per_launch,
+           "groups_in_flight": ft.PipelinedGroups(),
            "template_edge_counts": {str(k): v for k, v in counts.items()}, "clocks": clk,
            "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak,
                         "achieved": total_bytes / (ms * 1e-3) / 1e9,
@@ -758,6 +761,8 @@ def run_ours(args, world, rank, local):
     from fastfft_b200.autotune import tune
 
     per_launch = tune(ft, ins, images[0], outs)
+    groups = ft.PipelinedGroups()
+    tuned = dict(tune.last_timings)
     step_no = [0]
     corr_size = ft.CorrelationSize()
 
@@ -1076,7 +1081,7 @@ def run_ours(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
             "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": ms / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config(B, corr_size, per_launch),
+            "config": config(B, corr_size, per_launch, groups, tuned),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": B * n_in * 4,
@@ -1100,12 +1105,13 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def run_profile_case(case, local):
+def run_profile_case(case, local, groups=1, per_launch=64):
     """A small fixed workload for ncu captures (no timing, no checks): one warm-up call and
     one profiled call.  "headline": 64 templates of 384^2 against one 4096^2 image spectrum,
     1024^2 windows (the bench's step: image preparation, R2C, fused column pass, C2R);
     "single": one FwdImageInvFFT call of that template at the size-4096 kernels;
-    "uneven": the 1024-template uneven batch's first 64 templates (FP32)."""
+    "uneven": the 1024-template uneven batch's first 64 templates (FP32).  groups / per_launch:
+    the headline case's schedule (groups in flight, templates per launch)."""
     import torch
 
     import fastfft_b200 as F
@@ -1147,7 +1153,8 @@ def run_profile_case(case, local):
         outputs = torch.empty(B, ft.ReturnInvOutputMemorySize(), device=dev)
         for _ in range(2):
             if case == "headline":
-                ft.SetTemplatesPerLaunch(64)
+                ft.SetPipelinedGroups(groups)
+                ft.SetTemplatesPerLaunch(per_launch)
                 ft.FwdImageInvFFTMany([templates[i] for i in range(B)], spec, [outputs[i] for i in range(B)])
             else:
                 ft.FwdImageInvFFT(templates[0], spec, outputs[0])
@@ -1171,9 +1178,12 @@ def main():
     ap.add_argument("--skip-uneven", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--profile-case", choices=["headline", "single", "uneven"],
                     help="run one small fixed workload for an ncu capture and exit")
+    ap.add_argument("--profile-groups", type=int, default=1, help="groups in flight of the headline profile case")
+    ap.add_argument("--profile-per-launch", type=int, default=64, help="templates per launch of that case")
     args = ap.parse_args()
     if args.profile_case:
-        run_profile_case(args.profile_case, int(os.environ.get("LOCAL_RANK", "0")))
+        run_profile_case(args.profile_case, int(os.environ.get("LOCAL_RANK", "0")), args.profile_groups,
+                         args.profile_per_launch)
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()

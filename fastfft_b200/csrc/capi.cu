@@ -237,9 +237,11 @@ void size_buffers(fastfft_plan_s* h) {
             }
             h->red_t1_stride = round_up((mx / 2 + 1) * h->pitch_a, 32);   // complex elements per template
             h->red_t2_stride = round_up((mx / 2 + 1) * h->pitch_b, 32);   // column output [kx][y]
+            // one set of template slices per group in flight
+            const long long slots = (long long)h->red_batch * (h->pipe_groups > 1 ? 2 : 1);
             h->off_c_t1 = h->off_c_spec + round_up(spec, 256);
-            h->off_c_t2 = h->off_c_t1 + h->red_batch * h->red_t1_stride * 8;
-            h->bytes_c = h->off_c_t2 + h->red_batch * h->red_t2_stride * 8;
+            h->off_c_t2 = h->off_c_t1 + slots * h->red_t1_stride * 8;
+            h->bytes_c = h->off_c_t2 + slots * h->red_t2_stride * 8;
         }
     }
 }
@@ -270,9 +272,30 @@ static void create_prep_stream(fastfft_plan_s* h) {
     h->prep_device = dev;
 }
 
+// Second stream and events of the pipelined template groups (created once, like the
+// preparation stream; left null on failure, and the groups then run on `stream` alone).
+static void create_pipe_stream(fastfft_plan_s* h) {
+    if (h->pipe_stream || !h->red_ok || h->pipe_groups < 2) return;
+    cudaStream_t s = nullptr;
+    cudaEvent_t f = nullptr, j = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&j, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (j) cudaEventDestroy(j);
+        if (f) cudaEventDestroy(f);
+        if (s) cudaStreamDestroy(s);
+        return;
+    }
+    h->pipe_stream = s;
+    h->pipe_fork = f;
+    h->pipe_join = j;
+}
+
 fastfft_status allocate(fastfft_plan_s* h) {
     size_buffers(h);
     create_prep_stream(h);
+    create_pipe_stream(h);
     const size_t need = (size_t)(h->bytes_a + h->bytes_b + h->bytes_c) + 256;
     if (h->buffer && h->buffer_bytes >= need) return FASTFFT_OK;
     if (h->buffer) {
@@ -635,6 +658,12 @@ fastfft_status fastfft_destroy(fastfft_handle h) {
         cudaEventDestroy(h->prep_join);
         cudaStreamDestroy(h->prep_stream);
     }
+    if (h->pipe_stream) {
+        cudaStreamSynchronize(h->pipe_stream);
+        cudaEventDestroy(h->pipe_fork);
+        cudaEventDestroy(h->pipe_join);
+        cudaStreamDestroy(h->pipe_stream);
+    }
     if (h->buffer) {
         cudaStreamSynchronize(h->stream);
         cudaFree(h->buffer);
@@ -900,10 +929,13 @@ static fastfft_status xcorr_one(fastfft_handle h, const void* input, const void*
 // carries the same Nx*Ny factor as the size-N one.
 static fastfft_status red_prepare_image_on(fastfft_handle h, const void* image_spectrum, int mx, int my);
 
-// Wait on `stream` for a preparation still running on the side stream.
+// Wait on `stream` (the plan's stream or, inside a pipelined call, the pipe stream) for a
+// preparation still running on the side stream.
 static fastfft_status join_prep(fastfft_handle h) {
-    if (!h->prep_join_pending) return FASTFFT_OK;
-    h->prep_join_pending = false;
+    const bool pipe = h->pipe_stream && h->stream == h->pipe_stream;
+    bool& pending = pipe ? h->prep_join_pending_pipe : h->prep_join_pending;
+    if (!pending) return FASTFFT_OK;
+    pending = false;
     const cudaError_t e = cudaStreamWaitEvent(h->stream, h->prep_join, 0);
     return e == cudaSuccess ? FASTFFT_OK : cuda_fail(h, e, "joining the image preparation");
 }
@@ -919,6 +951,12 @@ static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spec
     // spectrum), prepare on the side stream, record the join for the next column pass
     cudaError_t e = cudaEventRecord(h->prep_fork, h->stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(h->prep_stream, h->prep_fork, 0);
+    // with pipelined groups the pipe stream may still read the previous spectrum too (only
+    // once forked in this call: its earlier work is already ordered before `stream`)
+    if (e == cudaSuccess && h->pipe_active) {
+        e = cudaEventRecord(h->pipe_join, h->pipe_stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(h->prep_stream, h->pipe_join, 0);
+    }
     if (e != cudaSuccess) return cuda_fail(h, e, "forking the image preparation");
     cudaStream_t main_stream = h->stream;
     h->stream = h->prep_stream;
@@ -931,6 +969,7 @@ static fastfft_status red_prepare_image(fastfft_handle h, const void* image_spec
         return st != FASTFFT_OK ? st : cuda_fail(h, e, "joining the image preparation");
     }
     h->prep_join_pending = true;
+    h->prep_join_pending_pipe = h->pipe_groups > 1 && h->pipe_stream;
     if (st != FASTFFT_OK) join_prep(h);
     return st;
 }
@@ -972,11 +1011,12 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int mx, int my, int n, c
                                       const int* dims, void* const* outs, const fastfft_op* pre_op,
                                       const fastfft_op* intra_op, const fastfft_op* post_op,
                                       unsigned long long* peaks = nullptr, const int* slots = nullptr,
-                                      unsigned long long* mip = nullptr, int mip_base = 0) {
+                                      unsigned long long* mip = nullptr, int mip_base = 0, int slice0 = 0) {
     char* c0 = region_c(h);
     const float2* spec = reinterpret_cast<const float2*>(c0 + h->off_c_spec);
-    float2* t1 = reinterpret_cast<float2*>(c0 + h->off_c_t1);
-    float2* t2 = reinterpret_cast<float2*>(c0 + h->off_c_t2);
+    // template slices [slice0, slice0 + n) of region C (slice0 > 0: the second group in flight)
+    float2* t1 = reinterpret_cast<float2*>(c0 + h->off_c_t1) + (long long)slice0 * h->red_t1_stride;
+    float2* t2 = reinterpret_cast<float2*>(c0 + h->off_c_t2) + (long long)slice0 * h->red_t2_stride;
     const float2* tw = nullptr;
     cudaError_t e;
     prof_begin_call(h);
@@ -1118,12 +1158,48 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
     void* grp_out[kMaxBatch];
     int grp_dims[2 * kMaxBatch];
     int grp_slot[kMaxBatch];
+    // Pipelined groups: every second group runs on the pipe stream with the second set of
+    // template slices; the pipe stream is forked from `stream` before its first group and
+    // joined back before returning (also on errors).
+    const bool pipe = h->pipe_groups > 1 && h->pipe_stream != nullptr;
+    bool pipe_forked = false;
+    int group_no = 0;
+    auto run_group = [&](int mx, int my, int m) -> fastfft_status {
+        const bool second = pipe && (group_no++ & 1);
+        if (!second)
+            return red_xcorr_batch(h, mx, my, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op,
+                                   post_op, peaks, grp_slot, mip, mip_base, 0);
+        if (!pipe_forked) {
+            cudaError_t e = cudaEventRecord(h->pipe_fork, h->stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(h->pipe_stream, h->pipe_fork, 0);
+            if (e != cudaSuccess) return cuda_fail(h, e, "forking the pipelined groups");
+            pipe_forked = true;
+            h->pipe_active = true;
+        }
+        cudaStream_t main_stream = h->stream;
+        h->stream = h->pipe_stream;
+        fastfft_status s2 = red_xcorr_batch(h, mx, my, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op,
+                                            intra_op, post_op, peaks, grp_slot, mip, mip_base, h->red_batch);
+        h->stream = main_stream;
+        return s2;
+    };
+    auto join_pipe = [&](fastfft_status prior) -> fastfft_status {
+        if (!pipe_forked) return prior;
+        h->pipe_active = false;
+        cudaError_t e = cudaEventRecord(h->pipe_join, h->pipe_stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(h->stream, h->pipe_join, 0);
+        if (e != cudaSuccess) {
+            cudaStreamSynchronize(h->pipe_stream);
+            return prior != FASTFFT_OK ? prior : cuda_fail(h, e, "joining the pipelined groups");
+        }
+        return prior;
+    };
     for (int i = 0; i < n; i++) {
         if (done[i]) continue;
         const void* img = image_spectra[i];
         const int mx = cls_x[i], my = cls_y[i];
         st = red_prepare_image(h, img, mx, my);
-        if (st != FASTFFT_OK) return st;
+        if (st != FASTFFT_OK) return join_pipe(st);
         int m = 0;
         for (int k = i; k < n; k++) {
             if (done[k] || image_spectra[k] != img || cls_x[k] != mx || cls_y[k] != my) continue;
@@ -1137,19 +1213,17 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
             }
             done[k] = 1;
             if (++m == h->red_batch) {
-                st = red_xcorr_batch(h, mx, my, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op,
-                                     post_op, peaks, grp_slot, mip, mip_base);
-                if (st != FASTFFT_OK) return st;
+                st = run_group(mx, my, m);
+                if (st != FASTFFT_OK) return join_pipe(st);
                 m = 0;
             }
         }
         if (m > 0) {
-            st = red_xcorr_batch(h, mx, my, m, grp_in, dims ? grp_dims : nullptr, grp_out, pre_op, intra_op,
-                                 post_op, peaks, grp_slot, mip, mip_base);
-            if (st != FASTFFT_OK) return st;
+            st = run_group(mx, my, m);
+            if (st != FASTFFT_OK) return join_pipe(st);
         }
     }
-    return FASTFFT_OK;
+    return join_pipe(FASTFFT_OK);
 }
 
 fastfft_status fastfft_fwd_image_inv_many(fastfft_handle h, int n, const void* const* inputs,
@@ -1217,6 +1291,39 @@ fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n) {
             h->buffer_bytes = 0;
         }
     }
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_set_pipelined_groups(fastfft_handle h, int n) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (n != 1 && n != 2) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "pipelined groups must be 1 or 2");
+    if (n == h->pipe_groups) return FASTFFT_OK;
+    if (h->buffer) cudaStreamSynchronize(h->stream);   // earlier calls may still use the slices
+    h->pipe_groups = n;
+    h->prepared_image = nullptr;
+    h->validated = false;
+    if (h->fwd_set && h->inv_set) {
+        fastfft_status st = validate(h);
+        if (st != FASTFFT_OK) return st;
+        const size_t before = h->buffer_bytes;
+        size_buffers(h);
+        if (h->buffer && (size_t)(h->bytes_a + h->bytes_b + h->bytes_c) + 256 > before) {
+            cudaFree(h->buffer);
+            h->buffer = nullptr;
+            h->buffer_bytes = 0;
+        }
+        int n_dev = 0;
+        if (cudaGetDeviceCount(&n_dev) == cudaSuccess && n_dev > 0)
+            create_pipe_stream(h);
+        else
+            cudaGetLastError();
+    }
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_pipelined_groups(fastfft_handle h, int* n) {
+    if (!h || !n) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null argument");
+    *n = (h->pipe_groups > 1 && h->pipe_stream && h->red_ok && !h->force_full_size) ? 2 : 1;
     return FASTFFT_OK;
 }
 

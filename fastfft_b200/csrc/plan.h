@@ -85,6 +85,17 @@ struct fastfft_plan_s {
     int prep_device = -1;
     bool prep_join_pending = false;  // prep_join recorded and not yet waited on by `stream`
 
+    // Pipelined template groups (fastfft_set_pipelined_groups): with 2, consecutive groups of
+    // the reduced-size correlation alternate between `stream` and pipe_stream, each with its
+    // own slices of region C, so that one group's row passes overlap the other's column pass
+    // and each group's intermediates are small enough to stay in L2.  pipe_stream is forked
+    // from `stream` at the start of a call and joined back at its end.
+    int pipe_groups = 1;
+    cudaStream_t pipe_stream = nullptr;
+    cudaEvent_t pipe_fork = nullptr, pipe_join = nullptr;
+    bool prep_join_pending_pipe = false;  // prep_join not yet waited on by pipe_stream
+    bool pipe_active = false;             // pipe_stream forked in the current call, not yet joined
+
     // kernels launched through this handle (fastfft_launch_count)
     long long launches = 0;
 

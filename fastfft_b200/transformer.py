@@ -251,6 +251,16 @@ class FourierTransformer:
         self._check(self._lib.fastfft_templates_per_launch(self._h, ctypes.byref(v)))
         return v.value
 
+    def SetPipelinedGroups(self, n):
+        """1 or 2 groups of templates in flight in the batched reduced-size path (2: consecutive
+        groups alternate between two streams, each group's intermediates small enough for L2)."""
+        self._check(self._lib.fastfft_set_pipelined_groups(self._h, int(n)))
+
+    def PipelinedGroups(self):
+        v = ctypes.c_int()
+        self._check(self._lib.fastfft_pipelined_groups(self._h, ctypes.byref(v)))
+        return v.value
+
     def SetImageReuse(self, enable=True):
         """Declare that image spectra do not change while in use: the reduced spectrum prepared
         for an image address is reused by later calls naming the same address (single

@@ -192,6 +192,15 @@ FASTFFT_API void fastfft_decode_peak(unsigned long long key, float* value, unsig
 FASTFFT_API fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n);
 FASTFFT_API fastfft_status fastfft_templates_per_launch(fastfft_handle h, int* n);
 
+/* Groups of the batched reduced-size path in flight (1, the default, or 2).  With 2,
+ * consecutive groups of templates alternate between the plan's stream and a second stream
+ * of the plan, each with its own intermediate slices, so one group's row passes overlap the
+ * other's fused column pass and a group's intermediates can stay in L2; the call still
+ * completes in the plan's stream order.  No reference counterpart (the reference has no
+ * batched call). */
+FASTFFT_API fastfft_status fastfft_set_pipelined_groups(fastfft_handle h, int n);
+FASTFFT_API fastfft_status fastfft_pipelined_groups(fastfft_handle h, int* n);
+
 /* The batched call correlates at the smallest supported size M >= L + W - 1 per axis (a
  * power of two, or 3 * 2^k with 128 <= 2^k <= 2048) when that is below the plan's N (template in [0, L), window in [0, W)): every
  * retained lag then reads image pixels in [0, L + W - 1) only, so the size-M

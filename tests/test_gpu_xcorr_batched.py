@@ -244,3 +244,45 @@ def test_uneven_templates_use_their_own_size_class(torch_cuda):
         got = O.real_from_padded(host(o), iout)
         assert O.rel_l2(got, ref) <= RTOL_L2_FP32, (x, y)
         assert O.rel_max(got, ref) <= RTOL_MAX_FP32, (x, y)
+
+
+@pytest.mark.parametrize("per_launch", [1, 3, 5])
+def test_pipelined_groups_match_single_stream(torch_cuda, per_launch):
+    """Two groups in flight (alternating streams, own intermediate slices) give bit-identical
+    windows and peaks to one group in flight: interleaved images, uneven sizes (size classes,
+    one image preparation per class), an odd number of groups, and a CUDA graph replay."""
+    torch = torch_cuda
+    fmax, fout, iout = (96, 96, 1), (1024, 1024, 1), (128, 128, 1)
+    specs = [dev(torch, image_spectrum(fout, s).view(np.float32)) for s in (21, 22)]
+    rng = np.random.default_rng(23)
+    sizes = [(96, 96), (32, 32), (96, 96), (64, 48), (96, 96), (17, 95), (96, 80), (33, 33), (96, 96), (80, 20),
+             (96, 96)]
+    which = [0, 1, 0, 0, 1, 0, 1, 1, 0, 0, 1]
+    ins = [dev(torch, O.real_to_padded(rng.standard_normal((y, x)).astype(np.float32), (x, y, 1))) for x, y in sizes]
+    results = []
+    for groups in (1, 2):
+        ft = plan(fmax, fout, iout)
+        ft.SetTemplatesPerLaunch(per_launch)
+        ft.SetPipelinedGroups(groups)
+        assert ft.PipelinedGroups() == groups
+        outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in sizes]
+        peaks = torch.zeros(len(sizes), dtype=torch.int64, device="cuda")
+        ft.FwdImageInvFFTManySized(ins, sizes, [specs[w] for w in which], outs)
+        ft.FwdImageInvFFTManyPeaks(ins, [specs[w] for w in which], peaks, sizes=sizes)
+        graph_outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in sizes]
+        ft.FwdImageInvFFTManySized(ins, sizes, [specs[w] for w in which], graph_outs)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            ft.FwdImageInvFFTManySized(ins, sizes, [specs[w] for w in which], graph_outs)
+        for o in graph_outs:
+            o.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        del g
+        for a, b in zip(outs, graph_outs):
+            assert torch.equal(a, b)
+        results.append(([host(o) for o in outs], host(peaks)))
+    for a, b in zip(results[0][0], results[1][0]):
+        assert np.array_equal(a, b)
+    assert np.array_equal(results[0][1], results[1][1])
