@@ -691,21 +691,25 @@ def run_cufft(dev, images, templates, window0, corr, batch_full=16):
 def run_cufft_recipe(template, image_kykx, ours):
     """The reference's own cuFFT recipe (clip into the top-left of a zeroed 4096^2 buffer,
     in-place R2C, in-place C2R with a conj-multiply load callback, full 4096^2 output) as a
-    separate program (fastfft_b200/bin/cufft_recipe_bench, its own process so that it uses the
-    toolkit's cuFFT and nvJitLink), one template per execution as in the reference and 16 per
-    execution; the window of its output is compared with ours."""
+    separate program (fastfft_b200/csrc/comparator/cufft_recipe_bench.cu, statically linked
+    cuFFT for the callback, built here in a few seconds), one template per execution as in the
+    reference and 16 per execution; the window of its output is compared with ours."""
     import tempfile
 
-    exe = os.path.join(ROOT, "fastfft_b200", "bin", "cufft_recipe_bench")
-    fatbin = os.path.join(ROOT, "fastfft_b200", "bin", "cufft_recipe_cb.fatbin")
-    if not (os.path.exists(exe) and os.path.exists(fatbin)):
-        return {"unavailable": "comparator program not built (python -m fastfft_b200.build)"}
+    from fastfft_b200.build import build_comparator
+
+    try:
+        exe = build_comparator()
+    except RuntimeError as e:
+        return {"unavailable": "comparator build failed: " + str(e)[-200:]}
+    if exe is None:
+        return {"unavailable": "no static cuFFT in the toolkit"}
     out = {}
     with tempfile.TemporaryDirectory() as d:
         np.ascontiguousarray(template, dtype=np.float32).tofile(os.path.join(d, "template.f32"))
         np.ascontiguousarray(image_kykx, dtype=np.complex64).tofile(os.path.join(d, "image_kykx.c64"))
         for batch, reps in ((1, 40), (16, 6)):
-            p = subprocess.run([exe, d, str(N), str(L), str(batch), str(reps), fatbin, str(W)], capture_output=True,
+            p = subprocess.run([str(exe), d, str(N), str(L), str(batch), str(reps), str(W)], capture_output=True,
                                text=True, timeout=300)
             try:
                 r = json.loads(p.stdout.strip().splitlines()[-1])
@@ -716,8 +720,8 @@ def run_cufft_recipe(template, image_kykx, ours):
                 r = {"value": batch / (r["ms_per_execution"] * 1e-3), "unit": UNIT,
                      "rel_l2_vs_ours": float(np.linalg.norm(win - ours) / np.linalg.norm(ours))}
             out[f"templates_per_execution_{batch}"] = r
-    out["how"] = ("cuFFT 4096^2: clip into top-left, in-place R2C, in-place C2R with an LTO load callback "
-                  "conj(T) x I (the reference's padded_convolution_FastFFT_vs_cuFFT recipe), full output")
+    out["how"] = ("cuFFT 4096^2: clip into top-left, in-place R2C, in-place C2R with a load callback conj(T) x I "
+                  "(cufftXtSetCallback, the reference's padded_convolution_FastFFT_vs_cuFFT recipe), full output")
     return out
 
 

@@ -4,11 +4,11 @@
 // in-place cufftExecR2C, and an in-place cufftExecC2R whose load callback forms
 // conj(template) x image x scale (the recipe of src/tests/padded_convolution_FastFFT_vs_cuFFT.cu:317-378,
 // callback src/fastfft/Image.cu:315-343).  The full N x N output is written, as there.
-// The callback is an LTO callback (cufftXtSetJITCallback) compiled from cufft_recipe_cb.cu.
+// The callback is a device function pointer set with cufftXtSetCallback, as in the reference,
+// which needs the static cuFFT library (the program is built with -rdc and libcufft_static).
 //
-// A standalone program (its own process, so it uses the toolkit's cuFFT and nvJitLink, whose
-// versions match the LTO-IR of the callback, not the ones a Python process may have loaded):
-//   cufft_recipe_bench <dir> <n> <L> <batch> <reps> <fatbin> <rows>
+// A standalone program (its own process and its own statically linked cuFFT):
+//   cufft_recipe_bench <dir> <n> <L> <batch> <reps> <rows>
 // reads <dir>/template.f32 (L x L, row pitch L) and <dir>/image_kykx.c64 (N x (N/2+1)
 // complex64), correlates `batch` copies of the template per execution, times `reps`
 // executions with CUDA events after a warm-up and writes the first template's correlation
@@ -31,6 +31,20 @@ struct CmpConjMulParams {
     float scale;
 };
 
+// Load callback of the C2R: conj(template spectrum) x image spectrum x scale, the product of
+// the reference's CB_complexConjMulLoad_32f (src/fastfft/Image.cu:315-325 with
+// ComplexConjMulAndScale, include/detail/device_functions.h:10-15).
+__device__ cufftComplex conj_mul_load(void* data_in, size_t offset, void* caller_info, void* shared_ptr) {
+    const CmpConjMulParams* p = static_cast<const CmpConjMulParams*>(caller_info);
+    const cufftComplex t = static_cast<const cufftComplex*>(data_in)[offset];
+    const cufftComplex im = p->image[offset % p->image_elems];
+    cufftComplex r;
+    r.x = p->scale * (t.x * im.x + t.y * im.y);
+    r.y = p->scale * (t.x * im.y - t.y * im.x);
+    return r;
+}
+__device__ cufftCallbackLoadC d_conj_mul_load = conj_mul_load;
+
 struct Recipe {
     int n = 0, batch = 0;
     cufftHandle fwd = 0, inv = 0;
@@ -52,7 +66,7 @@ __global__ void clip_into_top_left(const float* __restrict__ in, int L, long lon
 
 
 
-int create(Recipe* r, int n, int batch, const void* fatbin, size_t fatbin_size) {
+int create(Recipe* r, int n, int batch) {
     r->n = n;
     r->batch = batch;
     int dims[2] = {n, n};
@@ -60,16 +74,17 @@ int create(Recipe* r, int n, int batch, const void* fatbin, size_t fatbin_size) 
     if (cudaMalloc(&r->d_params, sizeof(CmpConjMulParams)) != cudaSuccess) return 2;
     size_t ws = 0;
     if (cufftCreate(&r->fwd) != CUFFT_SUCCESS || cufftCreate(&r->inv) != CUFFT_SUCCESS) return 3;
-    if (cufftMakePlanMany(r->fwd, 2, dims, inembed, 1, n * (n + 2), cembed, 1, n * (n / 2 + 1), CUFFT_R2C, batch,
-                          &ws) != CUFFT_SUCCESS)
-        return 4;
+    cufftResult cr = cufftMakePlanMany(r->fwd, 2, dims, inembed, 1, n * (n + 2), cembed, 1, n * (n / 2 + 1),
+                                       CUFFT_R2C, batch, &ws);
+    if (cr != CUFFT_SUCCESS) return 400 + (int)cr;
+    cr = cufftMakePlanMany(r->inv, 2, dims, cembed, 1, n * (n / 2 + 1), inembed, 1, n * (n + 2), CUFFT_C2R, batch,
+                           &ws);
+    if (cr != CUFFT_SUCCESS) return 500 + (int)cr;
+    cufftCallbackLoadC h_cb = nullptr;
+    if (cudaMemcpyFromSymbol(&h_cb, d_conj_mul_load, sizeof(h_cb)) != cudaSuccess) return 6;
     void* info = r->d_params;
-    cufftResult cr = cufftXtSetJITCallback(r->inv, "cmp_conj_mul_load", fatbin, fatbin_size, CUFFT_CB_LD_COMPLEX,
-                                           &info);
+    cr = cufftXtSetCallback(r->inv, reinterpret_cast<void**>(&h_cb), CUFFT_CB_LD_COMPLEX, &info);
     if (cr != CUFFT_SUCCESS) return 100 + (int)cr;
-    if (cufftMakePlanMany(r->inv, 2, dims, cembed, 1, n * (n / 2 + 1), inembed, 1, n * (n + 2), CUFFT_C2R, batch,
-                          &ws) != CUFFT_SUCCESS)
-        return 5;
     return 0;
 }
 
@@ -102,16 +117,15 @@ int fail(const char* what, int code) {
 }  // namespace
 
 int main(int argc, char** argv) {
-    if (argc < 8) return fail("usage: cufft_recipe_bench <dir> <n> <L> <batch> <reps> <fatbin> <rows>", 2);
+    if (argc < 7) return fail("usage: cufft_recipe_bench <dir> <n> <L> <batch> <reps> <rows>", 2);
     const std::string dir = argv[1];
     const int n = std::atoi(argv[2]), L = std::atoi(argv[3]), batch = std::atoi(argv[4]), reps = std::atoi(argv[5]);
-    const int rows = std::atoi(argv[7]);
+    const int rows = std::atoi(argv[6]);
     if (n < 16 || L < 1 || L > n || batch < 1 || reps < 1 || rows < 1 || rows > n) return fail("bad arguments", 2);
-    const std::vector<char> fatbin = read_all(argv[6]);
     const std::vector<char> tpl = read_all((dir + "/template.f32").c_str());
     const std::vector<char> img = read_all((dir + "/image_kykx.c64").c_str());
     const size_t img_bytes = (size_t)n * (n / 2 + 1) * 8;
-    if (fatbin.empty() || tpl.size() != (size_t)L * L * 4 || img.size() != img_bytes) return fail("inputs", 3);
+    if (tpl.size() != (size_t)L * L * 4 || img.size() != img_bytes) return fail("inputs", 3);
     float* d_t = nullptr;
     void* d_img = nullptr;
     float* d_work = nullptr;
@@ -122,7 +136,7 @@ int main(int argc, char** argv) {
     cudaMemcpy(d_t, tpl.data(), tpl.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(d_img, img.data(), img_bytes, cudaMemcpyHostToDevice);
     Recipe r;
-    int rc = create(&r, n, batch, fatbin.data(), fatbin.size());
+    int rc = create(&r, n, batch);
     if (rc != 0) return fail("plan or callback", rc);
     // the reference scales by FT_normalization_factor^2; here 1, the unnormalised product
     CmpConjMulParams p{static_cast<const cufftComplex*>(d_img), (unsigned long long)n * (n / 2 + 1), 1.f};
