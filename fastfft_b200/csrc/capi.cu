@@ -139,10 +139,11 @@ fastfft_status validate(fastfft_plan_s* h) {
     }
     if (dim != h->rank) return fail(h, FASTFFT_ERR_INVALID_DIMS, "plan dimensionality does not match the handle rank");
     // transform lengths: powers of two (FastFFT.cu:895-927); real-input 2D plans also take
-    // 3 * 2^k with 128 <= 2^k <= 2048 (384 ... 6144), which the reference rejects
+    // 3 * 2^k with 128 <= 2^k <= 2048 (384 ... 6144) and 5 * 2^k with 128 <= 2^k <= 1024
+    // (640 ... 5120), which the reference rejects
     const bool wide = dim == 2 && !cplx_dtype(h->input_dtype);
-    auto len_ok = [&](long long v) { return is_pow2(v) || (wide && v <= 6144 && ffb::is_3p_size((int)v)); };
-    const char* lens = wide ? "powers of 2 or 3 * 2^k (384 ... 6144)" : "powers of 2";
+    auto len_ok = [&](long long v) { return is_pow2(v) || (wide && v <= 6144 && ffb::is_rp_size((int)v)); };
+    const char* lens = wide ? "powers of 2, 3 * 2^k (384 ... 6144) or 5 * 2^k (640 ... 5120)" : "powers of 2";
     if ((!len_ok(fi.x) || !len_ok(fi.y) || !is_pow2(fi.z)) && h->fwd_change != SizeChange::Increase)
         return fail(h, FASTFFT_ERR_INVALID_DIMS,
                     std::string("input dimensions must be ") + lens + " unless the forward transform pads");
@@ -174,12 +175,14 @@ long long pow2_at_least(long long v) {
 }
 
 // Smallest transform length >= v of the reduced-size correlation: a power of two, or
-// 3 * 2^k (kMinP3 <= 2^k <= kMaxP3) when that is shorter.
+// 3 * 2^k (kMinP3 <= 2^k <= kMaxP3) or 5 * 2^k (kMinP3 <= 2^k <= kMaxP5) when shorter.
 long long corr_size_at_least(long long v) {
     long long best = std::max<long long>(ffb::kMinN, pow2_at_least(v));
 #if FFB_ENABLE_FFT3
     for (long long p = ffb::kMinP3; p <= ffb::kMaxP3; p *= 2)
         if (3 * p >= v && 3 * p < best) best = 3 * p;
+    for (long long p = ffb::kMinP3; p <= ffb::kMaxP5; p *= 2)
+        if (5 * p >= v && 5 * p < best) best = 5 * p;
 #endif
     return best;
 }

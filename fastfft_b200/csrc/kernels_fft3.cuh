@@ -1,14 +1,15 @@
-// Pass kernels at the lengths N = 3P of the reduced-size correlation (sm_100a).
+// Pass kernels at the lengths N = RP (R = 3 or 5) of the reduced-size correlation and of the
+// 2D plans beyond powers of two (sm_100a).
 //
 // Same argument structures, data layouts and outputs as the power-of-two kernels in
-// kernels_2d.cuh / kernels_xcorr.cuh; only the FFT inside differs (length 3P, fft3.cuh):
+// kernels_2d.cuh / kernels_xcorr.cuh; only the FFT inside differs (length RP, fft3.cuh):
 //   r2c3_rows_kernel   : row R2C, two real rows per complex FFT, transposed [kx][y] output
 //   c2r3_rows_kernel   : row C2R from [kx][y], two rows per complex FFT, fused peak search
 //   cols3_kernel       : column FFT (2D layout), forward / inverse / fused correlation, keep W
 //   xcorr3_cols_kernel : batched fused column pass (TMA-staged image and template columns,
 //                        forward, conj(T) * I, inverse), keep W
 // Time-domain data are loaded and stored in natural order; the spectrum side is decimated
-// by 3 (thread (k2, j) holds X[3 (j + T' q) + k2]).
+// by R (thread (k2, j) holds X[R (j + T' q) + k2]).  R = 3 or 5 (lengths 3 * 2^k, 5 * 2^k).
 #pragma once
 
 #include "fft3.cuh"
@@ -31,15 +32,15 @@ constexpr int kXcorr3SmThreads = 384;
 #define FFB_ROWS3_MIN_BLOCKS 2
 #endif
 
-template <int P, class InT, int FPB>
-__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, FFB_ROWS3_MIN_BLOCKS)
+template <int R, int P, class InT, int FPB>
+__global__ void __launch_bounds__(FftRShape<R, P>::T * FPB, FFB_ROWS3_MIN_BLOCKS)
 r2c3_rows_kernel(RowFwdArgs a) {
-    using S3 = Fft3Shape<P>;
+    using S3 = FftRShape<R, P>;
     constexpr int N = S3::N;
     constexpr int T = S3::T;
     constexpr int TP = S3::TP;
     extern __shared__ float2 smem[];
-    using G = Fft3Group<P, FPB, false>;
+    using G = FftRGroup<R, P, FPB, false>;
     const int f = threadIdx.x / T;
     const int t = threadIdx.x - f * T;
     const int k2 = t / TP;
@@ -59,11 +60,11 @@ r2c3_rows_kernel(RowFwdArgs a) {
     const InT* pb = in_g + input_row(ra + 1, a.rows_y, a.rows_z) * in_pitch;
     float2* const out_g = a.out + (long long)gb * a.out_batch_stride;
     // two real rows as one complex sequence z[n] = a[n] + i b[n]; thread (r, j) holds
-    // z[3 (j + T' q) + r] (decimation in time: the sub-FFTs share the row's samples)
+    // z[R (j + T' q) + r] (decimation in time: the sub-FFTs share the row's samples)
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
-        const int n = 3 * (j + TP * q) + k2;
+        const int n = R * (j + TP * q) + k2;
         float xa = 0.f, xb = 0.f;
         if (n < L) {
             if (has_a) xa = ld_real<InT>(pa + n);
@@ -71,7 +72,7 @@ r2c3_rows_kernel(RowFwdArgs a) {
         }
         v[q] = make_float2(xa * a.scale, xb * a.scale);
     }
-    forward_dit<P>(v, g, j, t, a.tw, a.tw3, leading_slots_dit<P>(L, k2, j));
+    forward_dit<R, P>(v, g, j, t, a.tw, a.tw3, leading_slots_dit<R, P>(L, k2, j));
 
     // Split Z = A + iB into the two real-row spectra (every FFT's buffer is read by the
     // whole block): A[k] = (Z[k] + conj Z[N-k]) / 2, B[k] = -i (Z[k] - conj Z[N-k]) / 2.
@@ -89,8 +90,8 @@ r2c3_rows_kernel(RowFwdArgs a) {
     for (int it = 0; it < kItemsPerThread; it++, o += step) {
         const int k = k0 + T * it;
         if (k >= a.kmax) continue;
-        const float2 z1 = sf[loc3<P>(k)];
-        const float2 z2 = sf[loc3<P>(k == 0 ? 0 : N - k)];
+        const float2 z1 = sf[locR<R, P>(k)];
+        const float2 z2 = sf[locR<R, P>(k == 0 ? 0 : N - k)];
         const float2 A = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
         const float2 B = make_float2(0.5f * (z1.y + z2.y), 0.5f * (z2.x - z1.x));
         if (two) {
@@ -113,17 +114,17 @@ r2c3_rows_kernel(RowFwdArgs a) {
 
 // PLAIN: windows written at origin 0, no peak search, no projection (the epilogue is then
 // only the bounds check and the stores).
-template <int P, class OutT, int FPB, bool PLAIN>
-__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, FFB_C2R3_MIN_BLOCKS)
+template <int R, int P, class OutT, int FPB, bool PLAIN>
+__global__ void __launch_bounds__(FftRShape<R, P>::T * FPB, FFB_C2R3_MIN_BLOCKS)
 c2r3_rows_kernel(RowInvArgs a) {
-    using S3 = Fft3Shape<P>;
+    using S3 = FftRShape<R, P>;
     constexpr int N = S3::N;
     constexpr int T = S3::T;
     constexpr int TP = S3::TP;
     constexpr int H = N / 2;
     extern __shared__ float2 smem[];
-    using G = Fft3Group<P, FPB, false, S3::SUB_C2R, S3::C2R_FFT_EXTRA>;
-    // Z[k] of FFT ff goes to region k % 3 at phys(k / 3) (decimated by 3, so that sub-FFT k2
+    using G = FftRGroup<R, P, FPB, false, S3::SUB_C2R, S3::C2R_FFT_EXTRA>;
+    // Z[k] of FFT ff goes to region k % R at phys(k / R) (decimated by R, so that sub-FFT k2
     // finds its inputs Z[3 m + k2] contiguous in its own region)
     const int f = threadIdx.x / T;
     const int t = threadIdx.x - f * T;
@@ -159,14 +160,14 @@ c2r3_rows_kernel(RowInvArgs a) {
             }
         }
     }
-    // k % 3 and (N - k) % 3 stay fixed over the items (T = 3 T') and k / 3 moves by T' per
-    // item, so the divisions by 3 are done once.
+    // k % R and (N - k) % R stay fixed over the items (T = R T') and k / R moves by T' per
+    // item, so the divisions by R are done once.
     float2* const sf = smem + ff0 * G::STRIDE;
-    const int kq0 = k0 / 3, kr0 = k0 - 3 * (k0 / 3);
-    const int nq0 = (N - k0) / 3, nr0 = (N - k0) - 3 * ((N - k0) / 3);
+    const int kq0 = k0 / R, kr0 = k0 - R * (k0 / R);
+    const int nq0 = (N - k0) / R, nr0 = (N - k0) - R * ((N - k0) / R);
     float2* const s_k = sf + kr0 * G::SUB;
     float2* const s_nk = sf + nr0 * G::SUB;
-    static_assert((T * FPB) % FPB == 0 && T % 3 == 0, "item stride");
+    static_assert((T * FPB) % FPB == 0 && T % R == 0, "item stride");
 #pragma unroll
     for (int it = 0; it < kItemsPerThread; it++) {
         const int k = k0 + T * it;
@@ -195,7 +196,7 @@ c2r3_rows_kernel(RowInvArgs a) {
     OutT* ob = oa + a.out_pitch;
     const bool has_a = ra < a.n_rows, has_b = ra + 1 < a.n_rows;
     if constexpr (PLAIN) {
-        dit_output<P>(v, g, j, t, a.tw3, [&](int n, float2 x) {
+        dit_output<R, P>(v, g, j, t, a.tw3, [&](int n, float2 x) {
             if (n < a.W) {
                 if (has_a) st_real<OutT>(oa + n, x.x * a.scale);
                 if (has_b) st_real<OutT>(ob + n, x.y * a.scale);
@@ -207,7 +208,7 @@ c2r3_rows_kernel(RowInvArgs a) {
         unsigned long long best = 0;
         const unsigned int tmpl = (unsigned)(a.mip_base + a.peak_slot[gb]);
         unsigned long long* ma = a.mip ? a.mip + (long long)ra * a.W : nullptr;
-        dit_output<P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
+        dit_output<R, P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
             const int n = n0 - a.X0;
             if (n >= 0 && n < a.W) {
                 const float va = x.x * a.scale, vb = x.y * a.scale;
@@ -249,15 +250,15 @@ c2r3_rows_kernel(RowInvArgs a) {
 // cols_kernel is not supported at these lengths (3D transforms are powers of two).
 // ---------------------------------------------------------------------------
 // OutC: storage type of the forward spectrum (FWD mode; the other modes write float2)
-template <int P, int MODE, class InC, class ImgC, int FPB, class OutC = float2>
-__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB, Fft3Shape<P>::T * FPB < kXcorr3SmThreads
-                                                             ? kXcorr3SmThreads / (Fft3Shape<P>::T * FPB) : 1)
+template <int R, int P, int MODE, class InC, class ImgC, int FPB, class OutC = float2>
+__global__ void __launch_bounds__(FftRShape<R, P>::T * FPB, FftRShape<R, P>::T * FPB < kXcorr3SmThreads
+                                                                ? kXcorr3SmThreads / (FftRShape<R, P>::T * FPB) : 1)
 cols3_kernel(ColArgs a) {
-    using S3 = Fft3Shape<P>;
+    using S3 = FftRShape<R, P>;
     constexpr int T = S3::T;
     constexpr int TP = S3::TP;
     extern __shared__ float2 smem[];
-    using G = Fft3Group<P, FPB, true>;
+    using G = FftRGroup<R, P, FPB, true>;
     const int f = threadIdx.x / T;
     const int t = threadIdx.x - f * T;
     const int k2 = t / TP;
@@ -273,7 +274,7 @@ cols3_kernel(ColArgs a) {
         // spectrum X[k], k < L, natural order in the column: thread (k2, j) takes X[3 m + k2]
 #pragma unroll
         for (int q = 0; q < 16; q++) {
-            const int k = 3 * (j + TP * q) + k2;
+            const int k = R * (j + TP * q) + k2;
             const float2 x = (valid && k < a.L) ? ld_cplx<InC>(pin + k) : make_float2(0.f, 0.f);
             v[q] = (a.in_scale != 1.f) ? cscale(x, a.in_scale) : x;
         }
@@ -286,16 +287,19 @@ cols3_kernel(ColArgs a) {
 #pragma unroll
         for (int q = 0; q < 16; q++) {
             const int n1 = j + TP * q;
-            v[q] = dif_input<P>(ld(n1), ld(n1 + P), ld(n1 + 2 * P), n1, k2, a.tw3);
+            float2 x[R];
+#pragma unroll
+            for (int n2 = 0; n2 < R; n2++) x[n2] = ld(n1 + P * n2);
+            v[q] = dif_input<R, P>(x, n1, k2, a.tw3);
         }
-        BlockFft<P, false>::run(v, g, j, a.tw, valid ? leading_slots3<P>(a.L, j) : 0);
+        BlockFft<P, false>::run(v, g, j, a.tw, valid ? leading_slots_p<P>(a.L, j) : 0);
         if constexpr (MODE == COL_FWD) {
             // spectrum side: X[3 m + k2] straight from the registers
             if (valid) {
                 OutC* po = static_cast<OutC*>(a.out) + bz * a.out_batch_stride + (long long)col * a.out_stride;
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
-                    const int n = 3 * (j + TP * q) + k2 - a.W0;
+                    const int n = R * (j + TP * q) + k2 - a.W0;
                     if (n >= 0 && n < a.W) st_cplx<OutC>(po + n, (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q]);
                 }
             }
@@ -308,7 +312,7 @@ cols3_kernel(ColArgs a) {
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
                     float2 im = make_float2(0.f, 0.f);
-                    if (valid) im = ld_cplx_stream<ImgC>(pimg + 3 * (j + TP * q) + k2);
+                    if (valid) im = ld_cplx_stream<ImgC>(pimg + R * (j + TP * q) + k2);
                     const float2 pr = conj_mul(v[q], im);
                     v[q] = (sc != 1.f) ? cscale(pr, sc) : pr;
                 }
@@ -318,7 +322,7 @@ cols3_kernel(ColArgs a) {
     }
     // INV and XCORR: radix-3 output pass, natural order
     const int W = valid ? a.W : 0;
-    dit_output<P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
+    dit_output<R, P>(v, g, j, t, a.tw3, [&](int n0, float2 x) {
         const int n = n0 - a.W0;
         if (n >= 0 && n < W) pout[n] = (a.out_scale != 1.f) ? cscale(x, a.out_scale) : x;
     }, a.W0 + W);
@@ -333,10 +337,10 @@ cols3_kernel(ColArgs a) {
 // B200: 8.5 instead of 9.4 us per template for the 1536-point pass).
 constexpr bool kXcorr3DB = false;
 
-template <int P, class ImgC, int FPB>
+template <int R, int P, class ImgC, int FPB>
 struct Xcorr3Smem {
-    static constexpr int kImgBytes = 3 * P * (int)sizeof(ImgC);
-    static constexpr int kXchBytes = Fft3Group<P, FPB, kXcorr3DB>::BYTES;
+    static constexpr int kImgBytes = R * P * (int)sizeof(ImgC);
+    static constexpr int kXchBytes = FftRGroup<R, P, FPB, kXcorr3DB>::BYTES;
     static __host__ __device__ constexpr int t1_col_elems(int L) { return (L + 1) & ~1; }  // 16-byte multiple
     static __host__ __device__ constexpr int img_off() { return 0; }
     static __host__ __device__ constexpr int xch_off() { return (kImgBytes + 127) & ~127; }
@@ -350,13 +354,13 @@ struct Xcorr3Smem {
 
 // TC: the sub-FFTs' radix-16 passes on the tensor cores in BF16 split precision (fft_tc.cuh;
 // P = 512 only, where a sub-FFT is one warp)
-template <int P, class ImgC, int FPB, bool MUL, bool TC = false>
-__global__ void __launch_bounds__(Fft3Shape<P>::T * FPB,
-                                  Fft3Shape<P>::T * FPB < kXcorr3SmThreads ? kXcorr3SmThreads / (Fft3Shape<P>::T * FPB) : 1)
+template <int R, int P, class ImgC, int FPB, bool MUL, bool TC = false>
+__global__ void __launch_bounds__(FftRShape<R, P>::T * FPB,
+                                  FftRShape<R, P>::T * FPB < kXcorr3SmThreads ? kXcorr3SmThreads / (FftRShape<R, P>::T * FPB) : 1)
 xcorr3_cols_kernel(XcorrColArgs a) {
-    static_assert(!TC || P == 512, "tensor-core sub-FFTs are one warp (P = 512)");
-    using S3 = Fft3Shape<P>;
-    using SM = Xcorr3Smem<P, ImgC, FPB>;
+    static_assert(!TC || (R == 3 && P == 512), "tensor-core sub-FFTs: length 1536 (one warp per sub-FFT)");
+    using S3 = FftRShape<R, P>;
+    using SM = Xcorr3Smem<R, P, ImgC, FPB>;
     constexpr int T = S3::T;
     constexpr int TP = S3::TP;
     extern __shared__ __align__(128) unsigned char sm_raw[];
@@ -388,7 +392,7 @@ xcorr3_cols_kernel(XcorrColArgs a) {
 
     const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
     const int rounds = (nb + FPB - 1) / FPB;
-    Fft3Group<P, FPB, kXcorr3DB> grp(xch, f, k2);
+    FftRGroup<R, P, FPB, kXcorr3DB> grp(xch, f, k2);
     TcDft16 tc_f;
     if constexpr (TC) tc_f.init(j);
 #pragma unroll 1
@@ -419,25 +423,26 @@ xcorr3_cols_kernel(XcorrColArgs a) {
 #pragma unroll
             for (int q = 0; q < 16; q++) {
                 const int n1 = j + TP * q;
-                const float2 x0 = (live && n1 < Lg) ? src[n1] : make_float2(0.f, 0.f);
-                const float2 x1 = (live && n1 + P < Lg) ? src[n1 + P] : make_float2(0.f, 0.f);
-                const float2 x2 = (live && n1 + 2 * P < Lg) ? src[n1 + 2 * P] : make_float2(0.f, 0.f);
-                v[q] = dif_input<P>(x0, x1, x2, n1, k2, a.tw3);
+                float2 x[R];
+#pragma unroll
+                for (int n2 = 0; n2 < R; n2++)
+                    x[n2] = (live && n1 + P * n2 < Lg) ? src[n1 + P * n2] : make_float2(0.f, 0.f);
+                v[q] = dif_input<R, P>(x, n1, k2, a.tw3);
             }
         }
         if constexpr (TC)
             tc_fft512<false>(v, grp.begin(), tc_f, a.tw, j);
         else
-            BlockFft<P, false>::run(v, grp, j, a.tw, live ? leading_slots3<P>(Lg, j) : 0);
+            BlockFft<P, false>::run(v, grp, j, a.tw, live ? leading_slots_p<P>(Lg, j) : 0);
         if constexpr (MUL) {
             // CONJ_MUL (scale 1) skips the 32 multiplies of the scaling
             if (sc == 1.f) {
 #pragma unroll
-                for (int q = 0; q < 16; q++) v[q] = conj_mul(v[q], lds_cplx<ImgC>(img_s + 3 * (j + TP * q) + k2));
+                for (int q = 0; q < 16; q++) v[q] = conj_mul(v[q], lds_cplx<ImgC>(img_s + R * (j + TP * q) + k2));
             } else {
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
-                    const float2 im = lds_cplx<ImgC>(img_s + 3 * (j + TP * q) + k2);
+                    const float2 im = lds_cplx<ImgC>(img_s + R * (j + TP * q) + k2);
                     v[q] = cscale(conj_mul(v[q], im), sc);
                 }
             }
@@ -448,7 +453,7 @@ xcorr3_cols_kernel(XcorrColArgs a) {
             BlockFft<P, true>::run(v, grp, j, a.tw, 16);
         float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
         const int W = live ? a.W : 0;
-        dit_output<P>(v, grp, j, t, a.tw3, [&](int n, float2 x) {
+        dit_output<R, P>(v, grp, j, t, a.tw3, [&](int n, float2 x) {
             if (n < W) o[n] = x;
         }, a.W);
     }

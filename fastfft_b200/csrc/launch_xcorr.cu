@@ -44,12 +44,12 @@ static cudaError_t xcorr_v2_dispatch(int img_dtype, const XcorrColArgs& a, cudaS
 }
 
 cudaError_t launch_xcorr_cols(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st) {
-    if (is_3p_size(n)) return launch_xcorr3(n, img_dtype, a, st);
+    if (is_rp_size(n)) return launch_xcorr3(n, img_dtype, a, st);
     FFB_SIZE_SWITCH(n, xcorr_v2_dispatch, img_dtype, a, st)
 }
 
 size_t xcorr_cols_smem(int n, int img_dtype, int L, int n_batch) {
-    if (is_3p_size(n)) return xcorr3_smem(n, img_dtype, L, n_batch);
+    if (is_rp_size(n)) return xcorr3_smem(n, img_dtype, L, n_batch);
     const int isz = img_dtype == 3 ? 8 : 4;
     const int fpb = (n / 16) >= kXcorrBlockThreads ? 1 : kXcorrBlockThreads / (n / 16);
     const size_t img = ((size_t)n * isz + 127) & ~(size_t)127;

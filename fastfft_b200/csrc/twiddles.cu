@@ -52,16 +52,16 @@ static __global__ void init_twiddles_kernel(float2* tw) {
 }
 
 
-// Radix-3 pass tables of the lengths N = 3P: W_N^m = exp(-2 pi i m / N), m < 2P.
-static __global__ void init_twiddles3_kernel(float2* tw) {
+// Radix-R pass tables of the lengths N = RP: W_N^m = exp(-2 pi i m / N), m < (R - 1) P.
+static __global__ void init_twiddles_r_kernel(float2* tw, int r) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= kTw3Total) return;
-    for (int p = kMinP3; p <= kMaxP3; p *= 2) {
-        const int base = tw3_base(p);
-        if (gid < base + tw3_size_of(p)) {
+    if (gid >= twr_total(r)) return;
+    for (int p = kMinP3; p <= kMaxPR(r); p *= 2) {
+        const int base = twr_base(r, p);
+        if (gid < base + twr_size_of(r, p)) {
             const int m = gid - base;
-            // exp(-2 pi i m / 3p) = cospi(-x) + i sinpi(-x), x = 2 m / 3p
-            const double x = -2.0 * (double)m / (3.0 * (double)p);
+            // exp(-2 pi i m / rp) = cospi(-x) + i sinpi(-x), x = 2 m / rp
+            const double x = -2.0 * (double)m / ((double)r * (double)p);
             double sv, cv;
             sincospi(x, &sv, &cv);
             tw[gid] = make_float2((float)cv, (float)sv);
@@ -75,11 +75,13 @@ static __global__ void init_twiddles3_kernel(float2* tw) {
 // include/detail/device_functions.h:17-27).
 __device__ float2 g_twiddles[kTwTotal];
 __device__ float2 g_twiddles3[kTw3Total];
+__device__ float2 g_twiddles5[kTw5Total];
 
 namespace {
 std::mutex g_tw_mutex;
 const float2* g_tw_ptr[64] = {nullptr};
 const float2* g_tw3_ptr[64] = {nullptr};
+const float2* g_tw5_ptr[64] = {nullptr};
 }  // namespace
 
 cudaError_t twiddles_for(int n, const float2** out) {
@@ -91,9 +93,12 @@ cudaError_t twiddles_for(int n, const float2** out) {
     if (!g_tw_ptr[dev]) {
         void* p = nullptr;
         void* p3 = nullptr;
+        void* p5 = nullptr;
         e = cudaGetSymbolAddress(&p, g_twiddles);
         if (e != cudaSuccess) return e;
         e = cudaGetSymbolAddress(&p3, g_twiddles3);
+        if (e != cudaSuccess) return e;
+        e = cudaGetSymbolAddress(&p5, g_twiddles5);
         if (e != cudaSuccess) return e;
         cudaStream_t s;
         e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -101,7 +106,11 @@ cudaError_t twiddles_for(int n, const float2** out) {
         init_twiddles_kernel<<<(kTwTotal + 255) / 256, 256, 0, s>>>(static_cast<float2*>(p));
         e = cudaGetLastError();
         if (e == cudaSuccess) {
-            init_twiddles3_kernel<<<(kTw3Total + 255) / 256, 256, 0, s>>>(static_cast<float2*>(p3));
+            init_twiddles_r_kernel<<<(kTw3Total + 255) / 256, 256, 0, s>>>(static_cast<float2*>(p3), 3);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) {
+            init_twiddles_r_kernel<<<(kTw5Total + 255) / 256, 256, 0, s>>>(static_cast<float2*>(p5), 5);
             e = cudaGetLastError();
         }
         cudaError_t e2 = cudaStreamSynchronize(s);
@@ -110,9 +119,14 @@ cudaError_t twiddles_for(int n, const float2** out) {
         if (e2 != cudaSuccess) return e2;
         g_tw_ptr[dev] = static_cast<const float2*>(p);
         g_tw3_ptr[dev] = static_cast<const float2*>(p3);
+        g_tw5_ptr[dev] = static_cast<const float2*>(p5);
     }
     if (is_3p_size(n)) {
-        *out = g_tw3_ptr[dev] + tw3_base(n / 3);
+        *out = g_tw3_ptr[dev] + twr_base(3, n / 3);
+        return cudaSuccess;
+    }
+    if (is_5p_size(n)) {
+        *out = g_tw5_ptr[dev] + twr_base(5, n / 5);
         return cudaSuccess;
     }
     if (!is_pow2_size(n) || n < kMinN || n > kMaxN) return cudaErrorInvalidValue;

@@ -64,7 +64,10 @@ def test_memory_sizes_match_reference(fin, fout, iout):
     ((64, 64, 1), (512, 512, 1), (256, 256, 1), (256, 256, 1), C.ERR_INVALID_DIMS),  # fwd out != inv in
     ((64, 128, 1), (128, 64, 1), (128, 64, 1), (128, 64, 1), C.ERR_INVALID_DIMS),    # mixed grow/shrink
     ((100, 100, 1), (100, 100, 1), (100, 100, 1), (100, 100, 1), C.ERR_INVALID_DIMS),  # non-pow2, no pad
-    ((64, 64, 1), (320, 320, 1), (320, 320, 1), (320, 320, 1), C.ERR_INVALID_DIMS),  # 5 * 2^k fwd out
+    ((64, 64, 1), (320, 320, 1), (320, 320, 1), (320, 320, 1), C.ERR_INVALID_DIMS),  # 5 * 2^k below 640
+    ((64, 64, 1), (10240, 64, 1), (10240, 64, 1), (10240, 64, 1), C.ERR_INVALID_DIMS),  # 5 * 2^k above 5120
+    ((16, 16, 16), (320, 320, 320), (320, 320, 320), (320, 320, 320), C.ERR_INVALID_DIMS),  # 5 * 2^k in 3D
+    ((64, 64, 1), (448, 448, 1), (448, 448, 1), (448, 448, 1), C.ERR_INVALID_DIMS),  # 7 * 2^k
     ((64, 64, 1), (192, 192, 1), (192, 192, 1), (192, 192, 1), C.ERR_INVALID_DIMS),  # 3 * 2^k below 384
     ((16, 16, 16), (384, 384, 384), (384, 384, 384), (384, 384, 384), C.ERR_INVALID_DIMS),  # 3 * 2^k in 3D
     ((64, 64, 1), (512, 512, 1), (512, 512, 1), (600, 600, 1), C.ERR_INVALID_DIMS),  # inverse grows, non-pow2
@@ -85,6 +88,9 @@ def test_validation_rejects(fin, fout, iin, iout, status):
     ((1536, 1536, 1), (1536, 1536, 1), (700, 600, 1)),
     ((100, 200, 1), (768, 6144, 1), (768, 6144, 1)),
     ((1000, 10, 1), (3072, 32, 1), (3000, 20, 1)),
+    ((64, 64, 1), (640, 640, 1), (640, 640, 1)),
+    ((100, 200, 1), (1280, 5120, 1), (1280, 5120, 1)),
+    ((1000, 10, 1), (2560, 32, 1), (2000, 20, 1)),
 ])
 def test_three_times_power_of_two_lengths_accepted_in_2d(fin, fout, iout):
     ft = new()

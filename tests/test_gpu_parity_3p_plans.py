@@ -1,6 +1,7 @@
-"""2D plans at the lengths 3 * 2^k (384 ... 6144), which the reference rejects, against the
-FP64 oracle: forward, inverse (with a window origin), round trip, and the fused
-correlation through the size-N kernels (single call) and the reduced-size path (batched).
+"""2D plans at the lengths 3 * 2^k (384 ... 6144) and 5 * 2^k (640 ... 5120), which the
+reference rejects, against the FP64 oracle: forward, inverse (with a window origin), round
+trip, and the fused correlation through the size-N kernels (single call) and the
+reduced-size path (batched).
 """
 import numpy as np
 import pytest
@@ -26,6 +27,13 @@ FWD_CASES = [
     ((3072, 64, 1), (3072, 64, 1)),          # 3 * 2^k rows, power-of-two columns
     ((64, 6144, 1), (64, 6144, 1)),          # power-of-two rows, 6144-point columns
     ((1536, 768, 1), (384, 384, 1)),         # forward decrease: first outputs kept
+    ((640, 640, 1), (640, 640, 1)),           # 5 * 2^k
+    ((1280, 1280, 1), (1280, 1280, 1)),
+    ((100, 300, 1), (640, 2560, 1)),          # zero padding into 5 * 2^k on both axes
+    ((5120, 32, 1), (5120, 32, 1)),           # 5120-point rows
+    ((32, 5120, 1), (32, 5120, 1)),           # 5120-point columns
+    ((640, 1536, 1), (640, 1536, 1)),         # 5 * 2^k rows, 3 * 2^k columns
+    ((2560, 1280, 1), (640, 640, 1)),         # forward decrease
 ]
 
 
@@ -47,6 +55,9 @@ INV_CASES = [
     ((1536, 1536, 1), (1536, 1536, 1), (0, 0)),
     ((768, 3072, 1), (700, 1000, 1), (0, 0)),
     ((1536, 1536, 1), (700, 600, 1), (16, 32)),   # window away from the origin
+    ((1280, 1280, 1), (1280, 1280, 1), (0, 0)),
+    ((640, 2560, 1), (600, 2000, 1), (0, 0)),
+    ((2560, 640, 1), (1000, 500, 1), (40, 70)),
 ]
 
 
@@ -91,6 +102,45 @@ def test_correlation_at_1536(torch_cuda):
     ts = [random_real((150, 200), seed=79 + i) for i in range(3)]
     ft = make(fin, fout, iout)
     assert ft.CorrelationSize() == (1024, 768)
+    single = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    batched = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    ins = [dev(torch, O.real_to_padded(t, fin)) for t in ts]
+    for t, o in zip(ins, single):
+        ft.FwdImageInvFFT(t, d_spec, o)
+    ft.FwdImageInvFFTMany(ins, d_spec, batched)
+    p = O.Plan(fin, fout, fout, iout)
+    for t, a, b in zip(ts, single, batched):
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), spec, p, out_dtype=np.float64), iout)
+        for o in (a, b):
+            got = O.real_from_padded(host(o), iout)
+            assert O.rel_l2(got, ref) <= RTOL_L2_FP32
+            assert O.rel_max(got, ref) <= RTOL_MAX_FP32
+
+
+def test_round_trip_1280(torch_cuda):
+    torch = torch_cuda
+    fin = fout = (1280, 1280, 1)
+    x = random_real((1280, 1280), seed=81)
+    ft = make(fin, fout, fout)
+    n_max = max(ft.ReturnInputMemorySize(), ft.ReturnFwdOutputMemorySize())
+    buf = dev(torch, O.real_to_padded(x, fin), n_max)
+    ft.FwdFFT(buf)
+    ft.InvFFT(buf)
+    back = O.real_from_padded(host(buf), fout)[0]
+    assert O.rel_l2(back, x * 1280.0 * 1280.0) <= RTOL_L2_FP32
+
+
+def test_correlation_at_1280(torch_cuda):
+    """300 x 200 template, 1280^2 image, 900 x 700 window: single calls run the size-N
+    1280-point kernels, batched calls the reduced-size path (1280 x 1024 here)."""
+    torch = torch_cuda
+    fin, fout, iout = (300, 200, 1), (1280, 1280, 1), (900, 700, 1)
+    img = np.random.default_rng(82).standard_normal((1280, 1280))
+    spec = O.fwd(O.real_to_padded(img, fout, dtype=np.float64), fout, fout).astype(np.complex64)
+    d_spec = dev(torch, spec.view(np.float32))
+    ts = [random_real((200, 300), seed=83 + i) for i in range(3)]
+    ft = make(fin, fout, iout)
+    assert ft.CorrelationSize() == (1280, 1024)
     single = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
     batched = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
     ins = [dev(torch, O.real_to_padded(t, fin)) for t in ts]

@@ -1,8 +1,8 @@
-"""Batched correlation at the mixed-radix lengths 3 * 2^k against the FP64 oracle.
+"""Batched correlation at the mixed-radix lengths 3 * 2^k and 5 * 2^k against the FP64 oracle.
 
-When 3 * 2^k (2^k in [128, 2048]) reaches L + W - 1 before the next power of two, the
-batched call correlates at that length (three radix-16 sub-FFTs and a radix-3 pass per
-transform).  These tests drive every such length along each axis through all four
+When 3 * 2^k (2^k in [128, 2048]) or 5 * 2^k (2^k in [128, 1024]) reaches L + W - 1 before
+the next power of two, the batched call correlates at that length (three or five radix-16
+sub-FFTs and a radix-3 or radix-5 pass per transform).  These tests drive every such length along each axis through all four
 kernels that have a 3 * 2^k form (row R2C, fused column pass, row C2R, and the forward
 column pass of the image preparation) and compare the retained windows with the size-N
 correlation that the reference defines.
@@ -47,7 +47,19 @@ CASES3 = [
 ]
 
 
-@pytest.mark.parametrize("fin,fout,iout,msize", CASES3)
+CASES5 = [
+    ((128, 128, 1), (1024, 1024, 1), (512, 512, 1), (640, 640)),        # 639 -> 5 * 128
+    ((300, 300, 1), (2048, 2048, 1), (900, 900, 1), (1280, 1280)),      # 1199 -> 5 * 256
+    ((300, 200, 1), (2048, 1024, 1), (500, 600, 1), (1024, 1024)),      # 799 -> 1024, 799 -> 1024 (x), 5 * 2^k only where shorter
+    ((1000, 16, 1), (4096, 64, 1), (1500, 16, 1), (2560, 32)),          # 2499 -> 5 * 512 along x
+    ((16, 1000, 1), (64, 4096, 1), (16, 1500, 1), (32, 2560)),          # ... along y
+    ((2000, 8, 1), (8192, 32, 1), (3000, 8, 1), (5120, 16)),            # 4999 -> 5 * 1024 along x
+    ((8, 2000, 1), (32, 8192, 1), (8, 3000, 1), (16, 5120)),            # ... along y
+    ((200, 150, 1), (1024, 1024, 1), (440, 600, 1), (640, 768)),        # 639 -> 5 * 128, 749 -> 3 * 256
+]
+
+
+@pytest.mark.parametrize("fin,fout,iout,msize", CASES3 + CASES5)
 def test_mixed_radix_sizes_match_oracle(torch_cuda, fin, fout, iout, msize):
     torch = torch_cuda
     ft = plan(fin, fout, iout)
