@@ -94,7 +94,7 @@ def pass_bytes_per_template(corr, t_xy, w_xy, per_launch, n_per_call, t_size=4, 
     return [r2c, cols, c2r, prep]
 
 
-def config(templates_per_step, corr_size=None, per_launch=None, groups=None, tuned=None):
+def config(templates_per_step, corr_size=None, per_launch=None, groups=None, tuned=None, per_block=None):
     return {
         "workload": "2D fused cross-correlation FP32: 384^2 template zero-padded to 4096^2, conj-multiply with a "
                     "resident 4096^2 image spectrum, inverse cropped to a 1024^2 window",
@@ -103,6 +103,7 @@ def config(templates_per_step, corr_size=None, per_launch=None, groups=None, tun
         "correlation_size": list(corr_size) if corr_size else None,
         "templates_per_launch": per_launch,
         "groups_in_flight": groups,
+        "templates_per_block": per_block,
         "autotune_ms_per_step": tuned,
         "image_spectra": N_IMAGES,
         "l2": "3 image spectra of 67 MB per GPU rotate step by step (201 MB > 126 MB L2): each step reads its "
@@ -370,7 +371,8 @@ def run_uneven(dev, image_f32, storage, local, min_seconds, check=True):
                        "4096^2 image spectrum, 512^2 windows; the whole batch is one CUDA graph launch",
            "storage": storage, "value": UNEVEN_N_TEMPLATES / (ms * 1e-3), "unit": UNIT, "ms_per_batch": ms,
            "timed_batches": reps, "correlation_size": list(ft.CorrelationSize()), "templates_per_launch": per_launch,
-           "groups_in_flight": ft.PipelinedGroups(),
+           "groups_in_flight": ft.PipelinedGroups(), "templates_per_block": ft.TemplatesPerBlock(),
+           "autotune_ms_per_batch": dict(tune.last_timings),
            "template_edge_counts": {str(k): v for k, v in counts.items()}, "clocks": clk,
            "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak,
                         "achieved": total_bytes / (ms * 1e-3) / 1e9,
@@ -766,6 +768,7 @@ def run_ours(args, world, rank, local):
 
     per_launch = tune(ft, ins, images[0], outs)
     groups = ft.PipelinedGroups()
+    per_block = ft.TemplatesPerBlock()
     tuned = dict(tune.last_timings)
     step_no = [0]
     corr_size = ft.CorrelationSize()
@@ -1085,7 +1088,7 @@ def run_ours(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
             "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": ms / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config(B, corr_size, per_launch, groups, tuned),
+            "config": config(B, corr_size, per_launch, groups, tuned, per_block),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": B * n_in * 4,

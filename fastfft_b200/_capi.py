@@ -67,6 +67,8 @@ SIGNATURES = {
                                                ctypes.POINTER(_vp), ctypes.POINTER(_vp), _op, _op, _op]),
     "fastfft_set_templates_per_launch": (_st, [Handle, ctypes.c_int]),
     "fastfft_set_pipelined_groups": (_st, [Handle, ctypes.c_int]),
+    "fastfft_set_templates_per_block": (_st, [Handle, ctypes.c_int]),
+    "fastfft_templates_per_block": (_st, [Handle, ctypes.POINTER(ctypes.c_int)]),
     "fastfft_pipelined_groups": (_st, [Handle, ctypes.POINTER(ctypes.c_int)]),
     "fastfft_set_image_reuse": (_st, [Handle, ctypes.c_int]),
     "fastfft_set_tensor_core_dft": (_st, [Handle, ctypes.c_int]),

@@ -41,8 +41,10 @@ using namespace ffb;
 // length my; measured best on B200 with 64 per launch: six at 1536 (= 3 * 512; 5.37 instead of
 // 5.47 us per template for that pass; 4, 5 and 8 were slower), four at 1024 (1.99 instead of
 // 2.06; 6 and 16 were slower), eight elsewhere (at 256: 0.23 against 0.29 with four)
-static inline int xcorr_tpb(int n, long long my) {
-    const int per_block = FFB_XCORR_TPB != 8 ? FFB_XCORR_TPB : my == 3 * 512 ? 6 : my == 1024 ? 4 : 8;
+// (fastfft_set_templates_per_block overrides it; the autotuner measures the candidates)
+static inline int xcorr_tpb(const fastfft_plan_s* h, int n, long long my) {
+    const int per_block = h->tpb_request > 0 ? h->tpb_request
+                          : FFB_XCORR_TPB != 8 ? FFB_XCORR_TPB : my == 3 * 512 ? 6 : my == 1024 ? 4 : 8;
     return per_block > 0 && n > per_block ? per_block : n;
 }
 
@@ -230,7 +232,7 @@ void size_buffers(fastfft_plan_s* h) {
             // templates per launch: bounded by the shared memory of the fused column kernel
             h->red_batch = h->red_batch_request;
             while (h->red_batch > 1 &&
-                   xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, xcorr_tpb(h->red_batch, my)) >
+                   xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, xcorr_tpb(h, h->red_batch, my)) >
                        226 * 1024)
                 h->red_batch--;
             if (xcorr_cols_smem((int)my, FASTFFT_DTYPE_C64, (int)h->fwd_in.y, 1) > 226 * 1024) {
@@ -1051,7 +1053,7 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int mx, int my, int n, c
     c.img = spec; c.img_stride = my;
     c.out = t2; c.out_pitch = h->pitch_b; c.out_batch = h->red_t2_stride; c.W = (int)h->inv_out.y;
     c.n_cols = mx / 2 + 1; c.n_batch = n;
-    c.tpb = xcorr_tpb(n, my);
+    c.tpb = xcorr_tpb(h, n, my);
     if (dims)
         for (int g = 0; g < n; g++) c.L_g[g] = dims[2 * g + 1];
     c.intra_kind = intra_op ? intra_op->kind : FASTFFT_OP_NOOP;
@@ -1294,6 +1296,35 @@ fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n) {
             h->buffer_bytes = 0;
         }
     }
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_set_templates_per_block(fastfft_handle h, int n) {
+    if (!h) return fail(nullptr, FASTFFT_ERR_INVALID_ARGUMENT, "null handle");
+    if (n < 0 || n > kMaxBatch)
+        return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "templates per block must be in [0, " + std::to_string(kMaxBatch) + "]");
+    if (h->buffer) cudaStreamSynchronize(h->stream);   // earlier calls may still use the slices
+    h->tpb_request = n;
+    h->validated = false;
+    if (h->fwd_set && h->inv_set) {
+        fastfft_status st = validate(h);
+        if (st != FASTFFT_OK) return st;
+        // the templates per launch follow (they shrink where shared memory needs it, and grow
+        // back to the request); a buffer too small for them is reallocated by the next call
+        const size_t before = h->buffer_bytes;
+        size_buffers(h);
+        if (h->buffer && (size_t)(h->bytes_a + h->bytes_b + h->bytes_c) + 256 > before) {
+            cudaFree(h->buffer);
+            h->buffer = nullptr;
+            h->buffer_bytes = 0;
+        }
+    }
+    return FASTFFT_OK;
+}
+
+fastfft_status fastfft_templates_per_block(fastfft_handle h, int* n) {
+    if (!h || !n) return fail(h, FASTFFT_ERR_INVALID_ARGUMENT, "null argument");
+    *n = (h->red_ok && !h->force_full_size) ? xcorr_tpb(h, h->red_batch, h->red_my) : 1;
     return FASTFFT_OK;
 }
 

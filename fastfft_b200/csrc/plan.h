@@ -68,6 +68,7 @@ struct fastfft_plan_s {
     long long prepared_mx = 0, prepared_my = 0;   // the size it was prepared at
     int red_batch = 16;             // templates per launch in the reduced-size path
     int red_batch_request = 16;     // fastfft_set_templates_per_launch (bounded by shared memory)
+    int tpb_request = 0;            // fastfft_set_templates_per_block (0: built-in choice per length)
     long long red_t1_stride = 0, red_t2_stride = 0;  // complex elements per template slice
     long long off_c_t1 = 0, off_c_t2 = 0;
     int* dev_err = nullptr;  // device status word of bounded waits (inside the work buffer)

@@ -251,6 +251,15 @@ class FourierTransformer:
         self._check(self._lib.fastfft_templates_per_launch(self._h, ctypes.byref(v)))
         return v.value
 
+    def SetTemplatesPerBlock(self, n):
+        """Templates one block of the batched fused column pass serves (0: the built-in choice)."""
+        self._check(self._lib.fastfft_set_templates_per_block(self._h, int(n)))
+
+    def TemplatesPerBlock(self):
+        v = ctypes.c_int()
+        self._check(self._lib.fastfft_templates_per_block(self._h, ctypes.byref(v)))
+        return v.value
+
     def SetPipelinedGroups(self, n):
         """1 or 2 groups of templates in flight in the batched reduced-size path (2: consecutive
         groups alternate between two streams, each group's intermediates small enough for L2)."""

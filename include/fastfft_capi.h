@@ -192,6 +192,12 @@ FASTFFT_API void fastfft_decode_peak(unsigned long long key, float* value, unsig
 FASTFFT_API fastfft_status fastfft_set_templates_per_launch(fastfft_handle h, int n);
 FASTFFT_API fastfft_status fastfft_templates_per_launch(fastfft_handle h, int* n);
 
+/* Templates that one block of the batched fused column pass stages and transforms (0, the
+ * default: a per-length choice measured on B200 -- 6 at length 1536, 4 at 1024, 8 elsewhere),
+ * and the value in effect for the plan's correlation size.  No reference counterpart. */
+FASTFFT_API fastfft_status fastfft_set_templates_per_block(fastfft_handle h, int n);
+FASTFFT_API fastfft_status fastfft_templates_per_block(fastfft_handle h, int* n);
+
 /* Groups of the batched reduced-size path in flight (1, the default, or 2).  With 2,
  * consecutive groups of templates alternate between the plan's stream and a second stream
  * of the plan, each with its own intermediate slices, so one group's row passes overlap the

@@ -286,3 +286,30 @@ def test_pipelined_groups_match_single_stream(torch_cuda, per_launch):
     for a, b in zip(results[0][0], results[1][0]):
         assert np.array_equal(a, b)
     assert np.array_equal(results[0][1], results[1][1])
+
+
+def test_templates_per_block_setting(torch_cuda):
+    """Every templates-per-block choice of the fused column pass gives bit-identical windows
+    (only the grouping of templates into blocks changes), at 1536 and at 640 points."""
+    torch = torch_cuda
+    for fin, fout, iout in (((384, 384, 1), (2048, 2048, 1), (1024, 1024, 1)),
+                            ((128, 128, 1), (1024, 1024, 1), (512, 512, 1))):
+        spec = dev(torch, image_spectrum(fout, 27).view(np.float32))
+        rng = np.random.default_rng(28)
+        ins = [dev(torch, O.real_to_padded(rng.standard_normal((fin[1], fin[0])).astype(np.float32), fin))
+               for _ in range(11)]
+        ref = None
+        for tpb in (0, 1, 2, 5, 16):
+            ft = plan(fin, fout, iout)
+            ft.SetTemplatesPerLaunch(11)
+            ft.SetTemplatesPerBlock(tpb)
+            if tpb:
+                assert ft.TemplatesPerBlock() == min(tpb, 11)
+            outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ins]
+            ft.FwdImageInvFFTMany(ins, spec, outs)
+            got = [host(o) for o in outs]
+            if ref is None:
+                ref = got
+            else:
+                for a, b in zip(ref, got):
+                    assert np.array_equal(a, b), tpb
