@@ -245,12 +245,15 @@ FASTFFT_API fastfft_status fastfft_correlation_size(fastfft_handle h, int dims[2
  * (out_x, out_y, 1) with a forward pad (or no change) and an inverse crop at the origin
  * (or no change): FP32 template rows of pitch 2*(in_x/2+1), a complex64 (float2) image
  * spectrum [kx][ky], an FP32 window of pitch 2*(out_x/2+1).
- * Limit: its two intermediate arrays live in one fixed device array of 24 MiB that
- * every GPU loading the library holds until exit; sizes with
+ * Limit: its two intermediate arrays live in one fixed device array of 24 MiB that every
+ * GPU the library's device code has been loaded on holds until exit; sizes with
  * (n_x/2+1) * (round_up(in_y,4) + round_up(out_y,4)) * 8 bytes above it are rejected
  * with FASTFFT_ERR_UNSUPPORTED (4096^2 with a 384-row template and a 1024-row window
- * fits).  The first call on a device looks up that array's address and builds the
- * twiddle table (it synchronises), so make it before any stream capture.  All calls share
+ * fits).  CUDA loads device code and data lazily, so the first call on a device is what
+ * places that array, the twiddle tables and the kernels on it; it also looks up the
+ * array's address and builds the twiddle tables (it synchronises).  Make one such call per
+ * device at start-up, before a memory pool claims the device's free memory and before any
+ * stream capture; later calls allocate nothing.  All calls share
  * the array and it keeps the last call's contents (every value a call reads is written
  * by that call first): calls that overlap on the GPU race.  cuda_stream NULL selects
  * cudaStreamPerThread.  Errors: fastfft_last_error(NULL). */
