@@ -259,14 +259,31 @@ __device__ __forceinline__ void dit_output(float2 (&v)[16], G& g, int j, int t, 
         const int n1 = t + S3::T * i;
         if (n1 < lim) {
             const int p = phys(n1);
-            float2 w[R];
-            twiddle_powers<R>(w, ld_tw(twr + n1));
-            float2 z[R];
-            z[0] = buf[p];
+            if constexpr (R == 3) {
+                const float2 a = buf[p];
+                const float2 w1 = ld_tw(twr + n1), w2 = cmul(w1, w1);  // one load: W^2n1 = (W^n1)^2
+                const float2 b = cmulc(buf[G::SUB + p], w1);
+                const float2 c = cmulc(buf[2 * G::SUB + p], w2);
+                // inverse DFT3 of (a, b, c), formed only where kept
+                const float2 s = cadd(b, c);
+                store(n1, cadd(a, s));
+                if (n1 + P < keep) {
+                    const float2 d = csub(b, c);
+                    const float2 m = make_float2(fmaf(-0.5f, s.x, a.x), fmaf(-0.5f, s.y, a.y));
+                    const float hx = kH3 * d.x, hy = kH3 * d.y;
+                    store(n1 + P, make_float2(m.x - hy, m.y + hx));
+                    if (n1 + 2 * P < keep) store(n1 + 2 * P, make_float2(m.x + hy, m.y - hx));
+                }
+            } else {
+                float2 w[R];
+                twiddle_powers<R>(w, ld_tw(twr + n1));
+                float2 z[R];
+                z[0] = buf[p];
 #pragma unroll
-            for (int k2 = 1; k2 < R; k2++) z[k2] = cmulc(buf[k2 * G::SUB + p], w[k2]);
-            const int count = (keep - n1 + P - 1) / P;   // outputs n1 + P n2 < keep
-            idftr_head<R>(z, count < R ? count : R, [&](int n2, float2 x) { store(n1 + P * n2, x); });
+                for (int k2 = 1; k2 < R; k2++) z[k2] = cmulc(buf[k2 * G::SUB + p], w[k2]);
+                const int count = (keep - n1 + P - 1) / P;   // outputs n1 + P n2 < keep
+                idftr_head<R>(z, count < R ? count : R, [&](int n2, float2 x) { store(n1 + P * n2, x); });
+            }
         }
     }
 }
