@@ -187,6 +187,19 @@ __device__ __forceinline__ float2 dif_input(const float2 (&x)[R], int n1, int k2
     return k2 == 0 ? y : cmul(y, ld_tw(twr + n1 * k2));
 }
 
+// The radix-3 form of dif_input with its three inputs as scalars (the form the 1536-point
+// fused column pass was tuned with; the array form cost that kernel a register).
+template <int P>
+__device__ __forceinline__ float2 dif_input3(float2 x0, float2 x1, float2 x2, int n1, int k2,
+                                             const float2* __restrict__ tw3) {
+    const float2 s = cadd(x1, x2);
+    if (k2 == 0) return cadd(x0, s);
+    const float2 d = csub(x1, x2);
+    const float2 m = make_float2(fmaf(-0.5f, s.x, x0.x), fmaf(-0.5f, s.y, x0.y));
+    const float hs = k2 == 1 ? -kH3 : kH3;  // -i h d for k2 = 1, +i h d for k2 = 2
+    return cmul(make_float2(fmaf(-hs, d.y, m.x), fmaf(hs, d.x, m.y)), ld_tw(tw3 + n1 * k2));
+}
+
 // Inverse DFT_R of z[0..R-1] (W_R = exp(+2 pi i / R)); the outputs n2 < count are handed to
 // out(n2, value) (the output pruning of the last pass).
 template <int R, class Out>

@@ -423,11 +423,18 @@ xcorr3_cols_kernel(XcorrColArgs a) {
 #pragma unroll
             for (int q = 0; q < 16; q++) {
                 const int n1 = j + TP * q;
-                float2 x[R];
+                if constexpr (R == 3) {
+                    const float2 x0 = (live && n1 < Lg) ? src[n1] : make_float2(0.f, 0.f);
+                    const float2 x1 = (live && n1 + P < Lg) ? src[n1 + P] : make_float2(0.f, 0.f);
+                    const float2 x2 = (live && n1 + 2 * P < Lg) ? src[n1 + 2 * P] : make_float2(0.f, 0.f);
+                    v[q] = dif_input3<P>(x0, x1, x2, n1, k2, a.tw3);
+                } else {
+                    float2 x[R];
 #pragma unroll
-                for (int n2 = 0; n2 < R; n2++)
-                    x[n2] = (live && n1 + P * n2 < Lg) ? src[n1 + P * n2] : make_float2(0.f, 0.f);
-                v[q] = dif_input<R, P>(x, n1, k2, a.tw3);
+                    for (int n2 = 0; n2 < R; n2++)
+                        x[n2] = (live && n1 + P * n2 < Lg) ? src[n1 + P * n2] : make_float2(0.f, 0.f);
+                    v[q] = dif_input<R, P>(x, n1, k2, a.tw3);
+                }
             }
         }
         if constexpr (TC)
