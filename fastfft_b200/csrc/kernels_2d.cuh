@@ -243,6 +243,11 @@ struct ColArgs {
     // (set by the launcher when the column is 16-byte aligned; err receives a timeout).
     int stage_img;
     int* err;
+    // Transposed output (out_elem_stride > 1) whose FPB columns of a block are consecutive in
+    // memory for every element: the block writes through shared memory so that consecutive
+    // threads store consecutive columns (FPB x 8 bytes contiguous per element instead of two
+    // columns per warp).  Set by the launcher when the addressing allows it.
+    int out_coalesce;
 };
 
 // Shared-memory plan of cols_kernel (bytes): the FFT groups' exchange buffers, then (when the
@@ -343,9 +348,31 @@ cols_kernel(ColArgs a) {
         }
         BlockFft<N, true>::run(v, g, j, a.tw, 16, qout);
     }
+    const int out_div = a.out_div > 0 ? a.out_div : 1;
+    const long long es = a.out_elem_stride > 0 ? a.out_elem_stride : 1;
+    if constexpr (FPB > 1) {
+        if (a.out_coalesce) {
+            // every group parks its column in its own buffer (natural order), then item i of
+            // the block stores element W0 + i / FPB of column c0 + i % FPB
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 16; q++) g.base[phys(j + T * q)] = v[q];
+            __syncthreads();
+            const int c0 = blockIdx.x * FPB;
+            const int cols_here = min(FPB, a.n_cols - c0);
+            OutC* pout0 = static_cast<OutC*>(a.out) + bz * a.out_batch_stride +
+                          (long long)(c0 / out_div) * a.out_stride + (long long)(c0 % out_div) * a.out_stride2;
+            for (int i = threadIdx.x; i < a.W * FPB; i += T * FPB) {
+                const int n = i / FPB, ff = i - n * FPB;
+                if (ff < cols_here) {
+                    const float2 x = smem[ff * G::STRIDE + phys(n + a.W0)];
+                    st_cplx<OutC>(pout0 + ff + n * es, (a.out_scale != 1.f) ? cscale(x, a.out_scale) : x);
+                }
+            }
+            return;
+        }
+    }
     if (valid) {
-        const int out_div = a.out_div > 0 ? a.out_div : 1;
-        const long long es = a.out_elem_stride > 0 ? a.out_elem_stride : 1;
         OutC* pout = static_cast<OutC*>(a.out) + bz * a.out_batch_stride + (long long)(col / out_div) * a.out_stride +
                      (long long)(col % out_div) * a.out_stride2;
 #pragma unroll

@@ -16,6 +16,12 @@ static cudaError_t cols_impl(const ColArgs& args, cudaStream_t st) {
     a.stage_img = MODE == COL_XCORR && FPB == 1 && a.intra_kind != 0 && a.img != nullptr &&
                   reinterpret_cast<uintptr_t>(a.img) % 16 == 0 && (a.img_stride * isz) % 16 == 0 &&
                   (a.img_batch_stride * isz) % 16 == 0;
+    // transposed output through shared memory when the block's FPB columns are consecutive in
+    // memory for every element: out_stride2 == 1 within a block that does not cross an
+    // out_div boundary, or consecutive columns one element apart (out_div 1, out_stride 1)
+    const int out_div = a.out_div > 0 ? a.out_div : 1;
+    a.out_coalesce = FPB > 1 && a.out_elem_stride > 1 &&
+                     ((out_div % FPB == 0 && a.out_stride2 == 1) || (out_div == 1 && a.out_stride == 1));
     const size_t smem = a.stage_img ? (size_t)CS::kStagedBytes : (size_t)CS::kXchBytes;
     static std::atomic<int> high_water[64];
     auto fn = cols_kernel<N, MODE, InC, ImgC, OutC, FPB>;
