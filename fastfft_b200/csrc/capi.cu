@@ -823,7 +823,7 @@ fastfft_status fastfft_tensor_core_dft_active(fastfft_handle h, int* active) {
     if (st != FASTFFT_OK) return st;
     fastfft_plan_s sized = *h;  // the buffer plan of the current settings, without touching h
     size_buffers(&sized);
-    *active = (h->tc_dft && sized.red_ok && !h->force_full_size && sized.red_my == 3 * 512) ? 1 : 0;
+    *active = (h->tc_dft && sized.red_ok && !h->force_full_size && sized.red_my == 3 * 512 && h->fwd_in.y <= 512) ? 1 : 0;
     return FASTFFT_OK;
 }
 
@@ -1086,6 +1086,14 @@ static fastfft_status red_xcorr_batch(fastfft_handle h, int mx, int my, int n, c
     return FASTFFT_OK;
 }
 
+// The reduced-size correlation is exact for the correlation functors only: with CONJ_MUL (or
+// CONJ_MUL_THEN_SCALE) every retained output is a lag of the correlation, which the smaller
+// transform computes exactly; with NOOP or SCALE the call is a round trip of the template,
+// whose outputs scale with the transform size, so those calls run at the plan's size.
+static bool correlation_op(const fastfft_op* intra_op) {
+    return intra_op && (intra_op->kind == FASTFFT_OP_CONJ_MUL || intra_op->kind == FASTFFT_OP_CONJ_MUL_THEN_SCALE);
+}
+
 fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const void* image_spectrum, void* output,
                                      const fastfft_op* pre_op, const fastfft_op* intra_op,
                                      const fastfft_op* post_op) {
@@ -1096,7 +1104,7 @@ fastfft_status fastfft_fwd_image_inv(fastfft_handle h, const void* input, const 
     void* out = output ? output : const_cast<void*>(input);
     // With image reuse declared, a single template also goes through the reduced-size path:
     // the image is prepared on the first call that names it and reused after that.
-    if (h->image_reuse && h->red_ok && !h->force_full_size)
+    if (h->image_reuse && h->red_ok && !h->force_full_size && correlation_op(intra_op))
         return xcorr_many(h, 1, &input, nullptr, &image_spectrum, &out, pre_op, intra_op, post_op);
     return xcorr_one(h, input, image_spectrum, out, pre_op, intra_op, post_op);
 }
@@ -1126,7 +1134,7 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
         cudaError_t e = cudaMemsetAsync(peaks, 0, sizeof(unsigned long long) * (size_t)n, h->stream);
         if (e != cudaSuccess) return cuda_fail(h, e, "clearing the peak array");
     }
-    if (!h->red_ok || h->force_full_size) {
+    if (!h->red_ok || h->force_full_size || !correlation_op(intra_op)) {
         for (int i = 0; i < n; i++) {
             void* out = reduce ? (outputs ? outputs[i] : nullptr)
                                : ((outputs && outputs[i]) ? outputs[i] : const_cast<void*>(inputs[i]));

@@ -38,6 +38,10 @@ cudaError_t launch_cols3_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t
 cudaError_t launch_cols3_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_xcorr3(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st);
 size_t xcorr3_smem(int n, int img_dtype, int L, int n_batch);
+// Tensor-core form of the batched fused column pass at length 1536 (kernels_tc.cuh): templates
+// of up to 512 rows, windows of up to 1536; launch_xcorr3 routes calls with a.tc set here.
+bool xcorr1536_tc_supported(const XcorrColArgs& a);
+cudaError_t launch_xcorr1536_tc(int img_dtype, const XcorrColArgs& a, cudaStream_t st);
 
 // Radial operations on square 2D half spectra (spectrum_ops.cu).
 struct RadialArgs;

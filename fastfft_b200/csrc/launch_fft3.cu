@@ -24,6 +24,7 @@ cudaError_t launch_cols3_xcorr(int n, int img_dtype, const ColArgs& a, cudaStrea
     return is_5p_size(n) ? launch_cols_xcorr_r<5>(n, img_dtype, a, st) : launch_cols_xcorr_r<3>(n, img_dtype, a, st);
 }
 cudaError_t launch_xcorr3(int n, int img_dtype, const XcorrColArgs& a, cudaStream_t st) {
+    if (n == 3 * 512 && a.tc && xcorr1536_tc_supported(a)) return launch_xcorr1536_tc(img_dtype, a, st);
     return is_5p_size(n) ? launch_xcorr_r<5>(n, img_dtype, a, st) : launch_xcorr_r<3>(n, img_dtype, a, st);
 }
 size_t xcorr3_smem(int n, int img_dtype, int L, int n_batch) {

@@ -208,10 +208,12 @@ FASTFFT_API fastfft_status fastfft_set_pipelined_groups(fastfft_handle h, int n)
 FASTFFT_API fastfft_status fastfft_pipelined_groups(fastfft_handle h, int* n);
 
 /* The batched call correlates at the smallest supported size M >= L + W - 1 per axis (a
- * power of two, or 3 * 2^k with 128 <= 2^k <= 2048) when that is below the plan's N (template in [0, L), window in [0, W)): every
- * retained lag then reads image pixels in [0, L + W - 1) only, so the size-M
- * circular correlation against the spectrum of the image cropped to [0, M) gives the
- * same values as the size-N one.  Each distinct image in a call is prepared once.
+ * power of two, 3 * 2^k or 5 * 2^k) when that is below the plan's N (template in [0, L),
+ * window in [0, W)): every retained lag then reads image pixels in [0, L + W - 1) only, so
+ * the size-M circular correlation against the spectrum of the image cropped to [0, M) gives
+ * the same values as the size-N one.  This holds for the correlation intra-ops (CONJ_MUL,
+ * CONJ_MUL_THEN_SCALE); calls with NOOP or SCALE (a round trip of the template, whose values
+ * scale with the transform size) run at N.  Each distinct image in a call is prepared once.
  * force != 0 selects the size-N kernels instead.  No reference counterpart (the
  * reference aborts on a forward increase with an inverse decrease, FastFFT.cu:673-679). */
 FASTFFT_API fastfft_status fastfft_set_full_size_correlation(fastfft_handle h, int force);
@@ -224,15 +226,18 @@ FASTFFT_API fastfft_status fastfft_set_full_size_correlation(fastfft_handle h, i
  * which forgets the prepared image).  Changing the plan, the stream or the plan's settings
  * also forgets it.  Default off.  No reference counterpart. */
 FASTFFT_API fastfft_status fastfft_set_image_reuse(fastfft_handle h, int enable);
-/* enable != 0 runs the radix-16 passes of the batched correlation's fused column pass on the
- * tensor cores in BF16 split precision (hi/lo parts, FP32 accumulation; about 1e-5 relative
- * L2 against FP64 instead of about 6e-7) where the pass has that form: correlation length
- * 3 * 512 = 1536 along y.  Every other pass and size keeps the FP32 CUDA-core FFTs.  It is
- * slower than the FP32 form on B200 (the FFT's butterflies cost less than the split matrix
- * products).  Default off.  No reference counterpart (the reference computes in FP32). */
+/* enable != 0 runs the batched correlation's fused column pass at length 1536 along y on the
+ * tensor cores (tcgen05.mma with FP32 accumulators in tensor memory): each column's forward
+ * FFT, image product and inverse FFT as a four-step 48 x 32 DFT whose four stages are
+ * BF16 split-precision matrix products (hi/lo parts, three products per stage; about 1e-5
+ * relative L2 against FP64 instead of about 6e-7 for the FP32 form).  Applies to templates of
+ * up to 512 rows with CONJ_MUL or CONJ_MUL_THEN_SCALE; every other pass and size keeps the
+ * FP32 CUDA-core FFTs.  Default off.  No reference counterpart (the reference computes in
+ * FP32). */
 FASTFFT_API fastfft_status fastfft_set_tensor_core_dft(fastfft_handle h, int enable);
-/* *active = 1 when the batched correlation of this plan runs tensor-core passes (the option
- * is on and the plan correlates at length 1536 along y), else 0. */
+/* *active = 1 when the batched correlation of this plan runs the tensor-core pass (the option
+ * is on, the plan correlates at length 1536 along y and its templates have at most 512
+ * rows), else 0. */
 FASTFFT_API fastfft_status fastfft_tensor_core_dft_active(fastfft_handle h, int* active);
 /* Transform size {x, y} that fastfft_fwd_image_inv_many uses for this plan. */
 FASTFFT_API fastfft_status fastfft_correlation_size(fastfft_handle h, int dims[2]);

@@ -85,3 +85,80 @@ def test_low_precision_image_with_tensor_core_passes(torch_cuda):
     p = O.Plan(FIN, FOUT, FOUT, IOUT)
     ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, FIN), spec_deq, p, out_dtype=np.float64), IOUT)
     assert O.rel_l2(O.real_from_padded(host(out), IOUT), ref) <= RTOL_L2_TC
+
+
+HEAD_FIN, HEAD_FOUT, HEAD_IOUT = (384, 384, 1), (2048, 2048, 1), (1024, 1024, 1)   # correlates at 1536^2
+
+
+def _plan(fin, fout, iout, tc):
+    ft = F.FourierTransformer()
+    ft.SetForwardFFTPlan(*fin, *fout)
+    ft.SetInverseFFTPlan(*fout, *iout)
+    ft.SetTensorCoreDFT(tc)
+    return ft
+
+
+def _blob_case(torch, seed):
+    img = O.gaussian_blob_image(HEAD_FOUT[0], n_blobs=12, seed=seed)
+    spec = O.image_spectrum_fp32(img)
+    return img, spec, dev(torch, spec.view(np.float32))
+
+
+@pytest.mark.parametrize("intra", ["conj_mul_then_scale", "noop"])
+def test_benchmark_shape_partial_work_item(torch_cuda, intra):
+    """384^2 templates and 1024^2 windows (the 1536^2 correlation of the benchmark workload), 6
+    templates: the tensor-core pass takes 4 templates per work item, so the second item is half
+    empty (CONJ_MUL_THEN_SCALE).  With NOOP the call is a round trip of the template, which the
+    reduced size would scale differently: it runs at the plan's size."""
+    torch = torch_cuda
+    img, spec, d_spec = _blob_case(torch, 51)
+    rng = np.random.default_rng(52)
+    ts = []
+    for i in range(6):
+        y0, x0 = rng.integers(0, 600, size=2)
+        ts.append((img[y0:y0 + 384, x0:x0 + 384] + 0.2 * rng.standard_normal((384, 384))).astype(np.float32))
+    op = F.KernelFunction.conj_mul_then_scale(0.125) if intra != "noop" else F.KernelFunction.noop()
+    oop = (O.OP_CONJ_MUL_THEN_SCALE, 0.125) if intra != "noop" else (O.OP_NOOP, 1.0)
+    tc, fp = _plan(HEAD_FIN, HEAD_FOUT, HEAD_IOUT, True), _plan(HEAD_FIN, HEAD_FOUT, HEAD_IOUT, False)
+    assert tc.TensorCoreDFTActive() and tc.CorrelationSize() == (1536, 1536)
+    d_ts = [dev(torch, O.real_to_padded(t, HEAD_FIN)) for t in ts]
+    out_tc = [empty(torch, tc.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    out_fp = [empty(torch, fp.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    tc.FwdImageInvFFTMany(d_ts, d_spec, out_tc, intra_op=op)
+    fp.FwdImageInvFFTMany(d_ts, d_spec, out_fp, intra_op=op)
+    torch.cuda.synchronize()
+    p = O.Plan(HEAD_FIN, HEAD_FOUT, HEAD_FOUT, HEAD_IOUT)
+    for t, a, b in zip(ts, out_tc, out_fp):
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, HEAD_FIN), spec, p, intra_op=oop,
+                                                 out_dtype=np.float64), HEAD_IOUT)
+        got_tc = O.real_from_padded(host(a), HEAD_IOUT)
+        assert O.rel_l2(got_tc, ref) <= RTOL_L2_TC
+        if intra != "noop":
+            assert O.peak(got_tc)[0] == O.peak(O.real_from_padded(host(b), HEAD_IOUT))[0] == O.peak(ref)[0]
+
+
+def test_uneven_template_rows_in_one_work_item(torch_cuda):
+    """Templates of 258..384 rows share the 1536-point class, so one work item mixes lengths
+    (the tensor-core pass zero-fills each template's rows beyond its own)."""
+    torch = torch_cuda
+    img, spec, d_spec = _blob_case(torch, 53)
+    rng = np.random.default_rng(54)
+    sizes = [(384, 384), (384, 300), (384, 262), (200, 384), (384, 333), (384, 258), (300, 300)]
+    ts = [rng.standard_normal((y, x)).astype(np.float32) for x, y in sizes]
+    ft = _plan(HEAD_FIN, HEAD_FOUT, HEAD_IOUT, True)
+    ins = [dev(torch, O.real_to_padded(t, (x, y, 1))) for t, (x, y) in zip(ts, sizes)]
+    outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    ft.FwdImageInvFFTManySized(ins, sizes, d_spec, outs)
+    torch.cuda.synchronize()
+    for t, (x, y), o in zip(ts, sizes, outs):
+        p = O.Plan((x, y, 1), HEAD_FOUT, HEAD_FOUT, HEAD_IOUT)
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, (x, y, 1)), spec, p, out_dtype=np.float64),
+                                 HEAD_IOUT)
+        assert O.rel_l2(O.real_from_padded(host(o), HEAD_IOUT), ref) <= RTOL_L2_TC, (x, y)
+
+
+def test_tall_templates_fall_back_to_fp32(torch_cuda):
+    """Templates of more than 512 rows (the tensor-core pass reads n < 512) run the FP32 pass."""
+    ft = _plan((64, 520, 1), (2048, 2048, 1), (64, 1000, 1), True)
+    assert ft.CorrelationSize()[1] == 1536
+    assert not ft.TensorCoreDFTActive()
