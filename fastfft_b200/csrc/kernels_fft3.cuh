@@ -13,7 +13,6 @@
 #pragma once
 
 #include "fft3.cuh"
-#include "fft_tc.cuh"
 #include "kernels_xcorr.cuh"
 
 namespace ffb {
@@ -352,13 +351,10 @@ struct Xcorr3Smem {
 };
 
 
-// TC: the sub-FFTs' radix-16 passes on the tensor cores in BF16 split precision (fft_tc.cuh;
-// P = 512 only, where a sub-FFT is one warp)
-template <int R, int P, class ImgC, int FPB, bool MUL, bool TC = false>
+template <int R, int P, class ImgC, int FPB, bool MUL>
 __global__ void __launch_bounds__(FftRShape<R, P>::T * FPB,
                                   FftRShape<R, P>::T * FPB < kXcorr3SmThreads ? kXcorr3SmThreads / (FftRShape<R, P>::T * FPB) : 1)
 xcorr3_cols_kernel(XcorrColArgs a) {
-    static_assert(!TC || (R == 3 && P == 512), "tensor-core sub-FFTs: length 1536 (one warp per sub-FFT)");
     using S3 = FftRShape<R, P>;
     using SM = Xcorr3Smem<R, P, ImgC, FPB>;
     constexpr int T = S3::T;
@@ -393,8 +389,6 @@ xcorr3_cols_kernel(XcorrColArgs a) {
     const float sc = a.intra_kind == 3 ? a.intra_scale : 1.f;
     const int rounds = (nb + FPB - 1) / FPB;
     FftRGroup<R, P, FPB, kXcorr3DB> grp(xch, f, k2);
-    TcDft16 tc_f;
-    if constexpr (TC) tc_f.init(j);
 #pragma unroll 1
     for (int it = 0; it < rounds; it++) {
         const int gl = it * FPB + f;                 // template within the block
@@ -437,10 +431,7 @@ xcorr3_cols_kernel(XcorrColArgs a) {
                 }
             }
         }
-        if constexpr (TC)
-            tc_fft512<false>(v, grp.begin(), tc_f, a.tw, j);
-        else
-            BlockFft<P, false>::run(v, grp, j, a.tw, live ? leading_slots_p<P>(Lg, j) : 0);
+        BlockFft<P, false>::run(v, grp, j, a.tw, live ? leading_slots_p<P>(Lg, j) : 0);
         if constexpr (MUL) {
             // CONJ_MUL (scale 1) skips the 32 multiplies of the scaling
             if (sc == 1.f) {
@@ -454,10 +445,7 @@ xcorr3_cols_kernel(XcorrColArgs a) {
                 }
             }
         }
-        if constexpr (TC)
-            tc_fft512<true>(v, grp.begin(), tc_f, a.tw, j);
-        else
-            BlockFft<P, true>::run(v, grp, j, a.tw, 16);
+        BlockFft<P, true>::run(v, grp, j, a.tw, 16);
         float2* o = a.out + (long long)g * a.out_batch + (long long)col * a.out_pitch;
         const int W = live ? a.W : 0;
         dit_output<R, P>(v, grp, j, t, a.tw3, [&](int n, float2 x) {

@@ -41,8 +41,8 @@ struct XcorrColArgs {
     int L_g[kMaxBatch];        // per-template valid rows of uneven batches (0: use L)
     int tpb;                   // templates per block: block (c, y) serves templates
                                // [y tpb, min((y + 1) tpb, n_batch)) of column c (grid.y blocks)
-    int tc;                    // 1: radix-16 passes on the tensor cores in BF16 split precision
-                               // where the kernel has that form (3P lengths with P = 512)
+    int tc;                    // 1: the tensor-core form of the pass where it has one (length 1536,
+                               // kernels_tc.cuh); otherwise the FP32 pass runs
 };
 
 // Shared-memory plan of the kernel (bytes), shared by the host launcher.

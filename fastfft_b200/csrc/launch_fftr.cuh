@@ -214,13 +214,10 @@ static cudaError_t xcorr3_impl(const XcorrColArgs& a0, cudaStream_t st) {
     XcorrColArgs a = a0;
     cudaError_t e = tables3(R, P, &a.tw, &a.tw3);
     if (e != cudaSuccess) return e;
-    static std::atomic<int> set_attr[4][64];
+    static std::atomic<int> set_attr[2][64];
     const bool mul = a.intra_kind != 0;
-    constexpr bool kTc = R == 3 && P == 512;   // the tensor-core form exists at length 1536
-    const bool tc = a.tc != 0 && kTc;
     auto fn = mul ? xcorr3_cols_kernel<R, P, ImgC, FPB, true> : xcorr3_cols_kernel<R, P, ImgC, FPB, false>;
-    if (tc) fn = mul ? xcorr3_cols_kernel<R, P, ImgC, FPB, true, kTc> : xcorr3_cols_kernel<R, P, ImgC, FPB, false, kTc>;
-    if ((e = ensure_smem_at_least((const void*)fn, (size_t)smem, set_attr[2 * tc + mul])) != cudaSuccess) return e;
+    if ((e = ensure_smem_at_least((const void*)fn, (size_t)smem, set_attr[mul])) != cudaSuccess) return e;
     fn<<<dim3(a.n_cols, (a.n_batch + a.tpb - 1) / a.tpb), FftRShape<R, P>::T * FPB, smem, st>>>(a);
     return cudaGetLastError();
 }
