@@ -412,8 +412,8 @@ def corr_size_for(edge, window):
 def run_storage(dev, images_f32, templates_f32, storage, steps, tc=False, warmup=3):
     """The headline workload with the templates and the image spectra stored in FP16 or
     BF16 (image spectra scaled by 1/4096 before rounding, the overflow guard), FP32
-    arithmetic and FP32 windows, optionally with the fused column pass's radix-16 stages on
-    the tensor cores in split precision; same steps as the main leg (B templates per step,
+    arithmetic and FP32 windows, optionally with the fused 1536-point column pass on the
+    tensor cores (tcgen05, BF16 split precision); same steps as the main leg (B templates per step,
     image spectra rotating).  Returns the result and, for the accuracy check, template 0's
     window with the dequantized template and image 0."""
     import torch
@@ -446,8 +446,8 @@ def run_storage(dev, images_f32, templates_f32, storage, steps, tc=False, warmup
     ft.FwdImageInvFFTMany(ins[:1], images[0], outs[:1])
     torch.cuda.synchronize()
     how = ("templates and image spectra stored in " + storage + " (image spectra scaled by 1/4096), FP32 windows; "
-           + ("the fused column pass's 16-point DFTs as BF16 hi/lo tensor-core products with FP32 accumulation"
-              if tc else "FP32 arithmetic"))
+           + ("the fused column pass as a tcgen05 four-step 48 x 32 DFT (BF16 hi/lo products, FP32 accumulation "
+              "in tensor memory)" if tc else "FP32 arithmetic"))
     result = {"storage": storage, "tensor_core_dft": bool(tc and ft.TensorCoreDFTActive()),
               "value": steps * B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
               "correlation_size": list(ft.CorrelationSize()), "templates_per_launch": per_launch, "how": how}
@@ -457,8 +457,9 @@ def run_storage(dev, images_f32, templates_f32, storage, steps, tc=False, warmup
 
 
 def run_tensor_core(dev, images, templates, steps, warmup=3):
-    """The headline workload (FP32 storage) with the fused column pass's radix-16 passes on
-    the tensor cores in BF16 split precision (SetTensorCoreDFT); same steps as the main leg.
+    """The headline workload (FP32 storage) with the fused 1536-point column pass on the tensor
+    cores (tcgen05 four-step 48 x 32 DFT in BF16 split precision, SetTensorCoreDFT); same steps
+    as the main leg.
     Returns the result and template 0's window against image 0 for the accuracy check."""
     import torch
 
@@ -488,8 +489,8 @@ def run_tensor_core(dev, images, templates, steps, warmup=3):
     result = {"value": steps * B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
               "active": ft.TensorCoreDFTActive(), "correlation_size": list(ft.CorrelationSize()),
               "templates_per_launch": per_launch,
-              "how": "FP32 storage; the fused column pass's 16-point DFTs as BF16 hi/lo matrix products "
-                     "(FP32 accumulation), everything else FP32"}
+              "how": "FP32 storage; the fused column pass as a tcgen05 four-step 48 x 32 DFT (BF16 hi/lo "
+                     "products, FP32 accumulation in tensor memory), everything else FP32"}
     return result, outputs[0].cpu().numpy()
 
 
@@ -1117,7 +1118,8 @@ def run_profile_case(case, local, groups=1, per_launch=64):
     one profiled call.  "headline": 64 templates of 384^2 against one 4096^2 image spectrum,
     1024^2 windows (the bench's step: image preparation, R2C, fused column pass, C2R);
     "single": one FwdImageInvFFT call of that template at the size-4096 kernels;
-    "uneven": the 1024-template uneven batch's first 64 templates (FP32).  groups / per_launch:
+    "uneven": the 1024-template uneven batch's first 64 templates (FP32); "headline_tc": the
+    headline case with the tensor-core column pass (SetTensorCoreDFT).  groups / per_launch:
     the headline case's schedule (groups in flight, templates per launch)."""
     import torch
 
@@ -1154,12 +1156,13 @@ def run_profile_case(case, local, groups=1, per_launch=64):
         ft = F.FourierTransformer()
         ft.SetForwardFFTPlan(L, L, 1, N, N, 1)
         ft.SetInverseFFTPlan(N, N, 1, W, W, 1)
-        B = 64 if case == "headline" else 1
+        ft.SetTensorCoreDFT(case == "headline_tc")
+        B = 1 if case == "single" else 64
         templates = torch.zeros(B, ft.ReturnInputMemorySize(), device=dev)
         templates.view(B, L, -1)[:, :, :L] = torch.randn(B, L, L, device=dev, generator=gen)
         outputs = torch.empty(B, ft.ReturnInvOutputMemorySize(), device=dev)
         for _ in range(2):
-            if case == "headline":
+            if case != "single":
                 ft.SetPipelinedGroups(groups)
                 ft.SetTemplatesPerLaunch(per_launch)
                 ft.FwdImageInvFFTMany([templates[i] for i in range(B)], spec, [outputs[i] for i in range(B)])
@@ -1183,7 +1186,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-cufft", action="store_true")
     ap.add_argument("--skip-uneven", action="store_true", help="skip the secondary workloads")
-    ap.add_argument("--profile-case", choices=["headline", "single", "uneven"],
+    ap.add_argument("--profile-case", choices=["headline", "headline_tc", "single", "uneven"],
                     help="run one small fixed workload for an ncu capture and exit")
     ap.add_argument("--profile-groups", type=int, default=1, help="groups in flight of the headline profile case")
     ap.add_argument("--profile-per-launch", type=int, default=64, help="templates per launch of that case")
