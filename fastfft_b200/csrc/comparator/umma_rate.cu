@@ -2,8 +2,9 @@
 // issues 1024 tcgen05.mma.kind::f16 (BF16 in, FP32 accumulate in tensor memory, K = 16, both
 // operands K-major in shared memory) from one thread and times them to completion with clock64;
 // prints cycles per instruction and MACs per cycle per SM for M in {64, 128}, N in {64..256},
-// one or several independent accumulators, and two operand layouts (no swizzle, 128-byte
-// swizzle).  The first shape is also checked against a host product.  Standalone program, not
+// one or several independent accumulators, two operand layouts (no swizzle, 128-byte swizzle),
+// and two ways of issuing (descriptors formed per MMA in a loop, or formed once with the K steps
+// unrolled).  The first shape is also checked against a host product.  Standalone program, not
 // part of the library:
 //   nvcc -gencode arch=compute_100a,code=sm_100a -O3 -o umma_rate umma_rate.cu && ./umma_rate
 #include <cuda_runtime.h>
@@ -41,8 +42,8 @@ __device__ __forceinline__ uint64_t make_desc(int layout, uint32_t addr, int kst
 constexpr int kReps = 256;   // x 4 K steps = 1024 MMAs per CTA
 
 __global__ void __launch_bounds__(128, 1)
-umma_rate_kernel(const uint16_t* A, const uint16_t* B, float* D, int layout, int M, int N, int nacc, int* err,
-                 unsigned long long* cycles) {
+umma_rate_kernel(const uint16_t* A, const uint16_t* B, float* D, int layout, int M, int N, int nacc, int fast,
+                 int* err, unsigned long long* cycles) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tbase;
@@ -75,7 +76,7 @@ umma_rate_kernel(const uint16_t* A, const uint16_t* B, float* D, int layout, int
     for (int pass = 0; pass < 2 && ok; pass++) {   // pass 0: one product (checked); pass 1: timed
         const int reps = pass == 0 ? 1 : kReps;
         const unsigned long long t0 = clock64();
-        if (tid == 0) {
+        if (tid == 0 && !fast) {
             for (int r = 0; r < reps; r++)
                 for (int s = 0; s < 4; s++) {
                     const uint32_t acc = (r >= nacc || s > 0) ? 1u : 0u;
@@ -85,9 +86,27 @@ umma_rate_kernel(const uint16_t* A, const uint16_t* B, float* D, int layout, int
                         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
                         "l"(make_desc(layout, saddr(As), s)), "l"(make_desc(layout, saddr(Bs), s)), "r"(idesc), "r"(acc));
                 }
+        } else if (tid == 0) {
+            // descriptors formed once, the four K steps unrolled, one accumulator
+            uint64_t da[4], db[4];
+            for (int s = 0; s < 4; s++) {
+                da[s] = make_desc(layout, saddr(As), s);
+                db[s] = make_desc(layout, saddr(Bs), s);
+            }
+            for (int r = 0; r < reps; r++) {
+#pragma unroll
+                for (int s = 0; s < 4; s++) {
+                    const uint32_t acc = (r > 0 || s > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                        "l"(da[s]), "l"(db[s]), "r"(idesc), "r"(acc));
+                }
+            }
+        }
+        if (tid == 0)
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(&mbar))
                          : "memory");
-        }
         ok = false;
         const unsigned long long g0 = now_ns();
         for (long long i = 0; i < (1ll << 22); i++) {   // bounded: 200 ms or 4M polls
@@ -163,10 +182,11 @@ int main() {
     cudaMemcpy(dB, b.data(), b.size() * 2, cudaMemcpyHostToDevice);
     const int smem = 16384 + 32768;
     cudaFuncSetAttribute(umma_rate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    struct Shape { int M, N, nacc; };
-    const Shape shapes[] = {{128, 64, 1}, {128, 64, 4}, {128, 96, 1}, {128, 128, 1}, {128, 128, 2},
-                            {128, 256, 1}, {128, 256, 2}, {64, 64, 1}, {64, 256, 1}};
-    printf("layout     M    N  accumulators  cycles/MMA  MAC/cycle/SM  (peak 4096)  check\n");
+    struct Shape { int M, N, nacc, fast; };
+    const Shape shapes[] = {{128, 64, 1, 0}, {128, 64, 4, 0}, {128, 96, 1, 0}, {128, 128, 1, 0}, {128, 128, 2, 0},
+                            {128, 256, 1, 0}, {128, 256, 2, 0}, {64, 64, 1, 0}, {64, 256, 1, 0},
+                            {128, 64, 1, 1}, {128, 96, 1, 1}, {128, 128, 1, 1}, {128, 256, 1, 1}};
+    printf("layout     M    N  accumulators  issue     cycles/MMA  MAC/cycle/SM (peak 4096)  check\n");
     int rc = 0;
     for (int layout = 0; layout < 2 && rc == 0; layout++)
         for (const Shape& s : shapes) {
@@ -174,7 +194,7 @@ int main() {
             cudaMemset(dD, 0, 128 * 64 * 4);
             cudaMemset(dErr, 0, 4);
             cudaMemset(dCyc, 0, 8);
-            umma_rate_kernel<<<sms, 128, smem>>>(dA, dB, dD, layout, s.M, s.N, s.nacc, dErr, dCyc);
+            umma_rate_kernel<<<sms, 128, smem>>>(dA, dB, dD, layout, s.M, s.N, s.nacc, s.fast, dErr, dCyc);
             const cudaError_t e = cudaDeviceSynchronize();
             int err = 0;
             unsigned long long cyc = 0;
@@ -200,8 +220,8 @@ int main() {
                 if (!(worst / scale < 1e-5)) rc = 2;
             }
             const double per = (double)cyc / sms / (kReps * 4);
-            printf("%-9s %4d %4d  %12d  %10.1f  %12.0f  %11s  %s\n", layout == 0 ? "no-swizzle" : "swizzle128", s.M, s.N,
-                   s.nacc, per, s.M * s.N * 16.0 / per, "", check);
+            printf("%-9s %4d %4d  %12d  %-8s  %10.1f  %12.0f  %11s  %s\n", layout == 0 ? "no-swizzle" : "swizzle128", s.M,
+                   s.N, s.nacc, s.fast ? "unrolled" : "loop", per, s.M * s.N * 16.0 / per, "", check);
         }
     cudaFree(dA);
     cudaFree(dB);
