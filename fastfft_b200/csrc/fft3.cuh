@@ -263,7 +263,7 @@ __device__ __forceinline__ void dit_output(float2 (&v)[16], G& g, int j, int t, 
     {
         float2* s = buf + g.r * G::SUB;
 #pragma unroll
-        for (int q = 0; q < 16; q++) s[phys(j + S3::TP * q)] = v[q];
+        for (int q = 0; q < 16; q++) s[phys_idx<S3::TP>(j, q)] = v[q];
     }
     g.sync_fft();
     const int lim = keep < P ? keep : P;
@@ -316,7 +316,7 @@ __device__ __forceinline__ float2* forward_dit(float2 (&v)[16], G& g, int j, int
     {
         float2* s = buf + g.r * G::SUB;
 #pragma unroll
-        for (int q = 0; q < 16; q++) s[phys(j + S3::TP * q)] = v[q];
+        for (int q = 0; q < 16; q++) s[phys_idx<S3::TP>(j, q)] = v[q];
     }
     g.sync_fft();
 #pragma unroll 2

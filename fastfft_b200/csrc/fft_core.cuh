@@ -342,6 +342,16 @@ constexpr int kMaxN = 8192;
 constexpr int kTwTotal = tw_base(kMaxN) + tw_size_of(kMaxN);
 
 __device__ __forceinline__ int phys(int i) { return i + (i >> 4); }
+// Padded-index step of a stride: for i0 and a stride d that is a multiple of 16 (or d = 1 and
+// i0 a multiple of 16, with q < 16), phys(i0 + q d) = phys(i0) + q phys_step(d) exactly; the
+// exchanges use it so each access is one base plus a constant offset.
+__host__ __device__ constexpr int phys_step(int d) { return d == 1 ? 1 : d + d / 16; }
+// phys(j + D q) for a compile-time stride D: base plus constant offsets when D % 16 == 0
+template <int D>
+__device__ __forceinline__ int phys_idx(int j, int q) {
+    if constexpr (D % 16 == 0) return phys(j) + q * phys_step(D);
+    else return phys(j + D * q);
+}
 
 // Twiddle tables (layout in FftShape) are generated in FP64 (sincospi) and rounded to
 // FP32 once; W_n^m = exp(-2 pi i m / n).
@@ -456,11 +466,19 @@ struct BlockFft {
             if (p < S::NP16 - 1 || S::REM > 1) {
                 float2* s = g.begin();
                 const int base = (j / ns) * 16 * ns + (j & (ns - 1));
+                // base is a multiple of 16 when ns = 1; ns and T are multiples of 16 otherwise
+                float2* const sw = s + phys(base);
 #pragma unroll
-                for (int r = 0; r < 16; r++) s[phys(base + r * ns)] = v[r];
+                for (int r = 0; r < 16; r++) sw[r * phys_step(ns)] = v[r];
                 g.sync();
+                if constexpr (T % 16 == 0) {
+                    const float2* const sr = s + phys(j);
 #pragma unroll
-                for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
+                    for (int q = 0; q < 16; q++) v[q] = sr[q * phys_step(T)];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 16; q++) v[q] = s[phys(j + T * q)];
+                }
             }
         }
         if constexpr (S::REM > 1) {
