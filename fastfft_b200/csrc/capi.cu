@@ -58,6 +58,14 @@ static inline int xcorr_tpb(const fastfft_plan_s* h, int n, long long my) {
 #ifndef FFB_ENABLE_FFT3
 #define FFB_ENABLE_FFT3 1
 #endif
+// Lengths 7 * 2^k among the reduced-size correlation's lengths (1), or not (0, the default):
+// a 7 * 2^k transform costs far more per point than the power of two above it (measured on
+// B200 in the uneven 1024-template batch, whose 384^2 templates with 512^2 windows would
+// correlate at 896 instead of 1024: 186,916 instead of 365,798 templates/s), so the
+// correlation uses 7 * 2^k lengths only when a plan's own N is one.
+#ifndef FFB_ENABLE_FFT7
+#define FFB_ENABLE_FFT7 0
+#endif
 
 namespace {
 
@@ -141,11 +149,13 @@ fastfft_status validate(fastfft_plan_s* h) {
     }
     if (dim != h->rank) return fail(h, FASTFFT_ERR_INVALID_DIMS, "plan dimensionality does not match the handle rank");
     // transform lengths: powers of two (FastFFT.cu:895-927); real-input 2D plans also take
-    // 3 * 2^k with 128 <= 2^k <= 2048 (384 ... 6144) and 5 * 2^k with 128 <= 2^k <= 1024
-    // (640 ... 5120), which the reference rejects
+    // 3 * 2^k with 128 <= 2^k <= 2048 (384 ... 6144), 5 * 2^k with 128 <= 2^k <= 1024
+    // (640 ... 5120) and 7 * 2^k with 128 <= 2^k <= 512 (896 ... 3584), which the reference
+    // rejects
     const bool wide = dim == 2 && !cplx_dtype(h->input_dtype);
     auto len_ok = [&](long long v) { return is_pow2(v) || (wide && v <= 6144 && ffb::is_rp_size((int)v)); };
-    const char* lens = wide ? "powers of 2, 3 * 2^k (384 ... 6144) or 5 * 2^k (640 ... 5120)" : "powers of 2";
+    const char* lens =
+        wide ? "powers of 2, 3 * 2^k (384 ... 6144), 5 * 2^k (640 ... 5120) or 7 * 2^k (896 ... 3584)" : "powers of 2";
     if ((!len_ok(fi.x) || !len_ok(fi.y) || !is_pow2(fi.z)) && h->fwd_change != SizeChange::Increase)
         return fail(h, FASTFFT_ERR_INVALID_DIMS,
                     std::string("input dimensions must be ") + lens + " unless the forward transform pads");
@@ -177,7 +187,8 @@ long long pow2_at_least(long long v) {
 }
 
 // Smallest transform length >= v of the reduced-size correlation: a power of two, or
-// 3 * 2^k (kMinP3 <= 2^k <= kMaxP3) or 5 * 2^k (kMinP3 <= 2^k <= kMaxP5) when shorter.
+// 3 * 2^k (kMinP3 <= 2^k <= kMaxP3) or 5 * 2^k (kMinP3 <= 2^k <= kMaxP5) when shorter (and
+// 7 * 2^k with FFB_ENABLE_FFT7).
 long long corr_size_at_least(long long v) {
     long long best = std::max<long long>(ffb::kMinN, pow2_at_least(v));
 #if FFB_ENABLE_FFT3
@@ -185,6 +196,10 @@ long long corr_size_at_least(long long v) {
         if (3 * p >= v && 3 * p < best) best = 3 * p;
     for (long long p = ffb::kMinP3; p <= ffb::kMaxP5; p *= 2)
         if (5 * p >= v && 5 * p < best) best = 5 * p;
+#if FFB_ENABLE_FFT7
+    for (long long p = ffb::kMinP3; p <= ffb::kMaxP7; p *= 2)
+        if (7 * p >= v && 7 * p < best) best = 7 * p;
+#endif
 #endif
     return best;
 }

@@ -1,4 +1,4 @@
-// Block FFTs of length N = R P (R = 3 or 5, P = 2^k) for sm_100a.
+// Block FFTs of length N = R P (R = 3, 5 or 7, P = 2^k) for sm_100a.
 //
 // These sizes exist for the reduced-size correlation and the 2D plans beyond powers of two:
 // the correlation's exact size only has to reach L + W - 1 per axis, and R * 2^k lands closer
@@ -28,6 +28,7 @@ namespace ffb {
 constexpr int kMinP3 = 128;
 constexpr int kMaxP3 = 2048;
 constexpr int kMaxP5 = 1024;   // 5 * 1024 = 5120 <= 8192, the longest transform of a plan
+constexpr int kMaxP7 = 512;    // 7 * 512 = 3584
 
 __host__ __device__ constexpr bool is_pow2_size(int n) { return n > 0 && (n & (n - 1)) == 0; }
 // N = 3P with a supported P
@@ -38,12 +39,18 @@ __host__ __device__ constexpr bool is_3p_size(int n) {
 __host__ __device__ constexpr bool is_5p_size(int n) {
     return n > 0 && n % 5 == 0 && is_pow2_size(n / 5) && n / 5 >= kMinP3 && n / 5 <= kMaxP5;
 }
-__host__ __device__ constexpr bool is_rp_size(int n) { return is_3p_size(n) || is_5p_size(n); }
+// N = 7P with a supported P
+__host__ __device__ constexpr bool is_7p_size(int n) {
+    return n > 0 && n % 7 == 0 && is_pow2_size(n / 7) && n / 7 >= kMinP3 && n / 7 <= kMaxP7;
+}
+__host__ __device__ constexpr bool is_rp_size(int n) { return is_3p_size(n) || is_5p_size(n) || is_7p_size(n); }
 // the radix R of a length R * 2^k (1 for a power of two)
-__host__ __device__ constexpr int radix_of(int n) { return is_3p_size(n) ? 3 : is_5p_size(n) ? 5 : 1; }
+__host__ __device__ constexpr int radix_of(int n) {
+    return is_3p_size(n) ? 3 : is_5p_size(n) ? 5 : is_7p_size(n) ? 7 : 1;
+}
 
 // Twiddles of the radix-R pass: W_RP^m = exp(-2 pi i m / RP), m < (R - 1) P, one block per P.
-__host__ __device__ constexpr int kMaxPR(int r) { return r == 3 ? kMaxP3 : kMaxP5; }
+__host__ __device__ constexpr int kMaxPR(int r) { return r == 3 ? kMaxP3 : r == 5 ? kMaxP5 : kMaxP7; }
 __host__ __device__ constexpr int twr_size_of(int r, int p) { return (r - 1) * p; }
 __host__ __device__ constexpr int twr_base(int r, int p) {
     int off = 0;
@@ -53,10 +60,11 @@ __host__ __device__ constexpr int twr_base(int r, int p) {
 __host__ __device__ constexpr int twr_total(int r) { return twr_base(r, kMaxPR(r)) + twr_size_of(r, kMaxPR(r)); }
 constexpr int kTw3Total = twr_total(3);
 constexpr int kTw5Total = twr_total(5);
+constexpr int kTw7Total = twr_total(7);
 
 template <int R, int P>
 struct FftRShape {
-    static_assert(R == 3 || R == 5, "radix 3 or 5");
+    static_assert(R == 3 || R == 5 || R == 7, "radix 3, 5 or 7");
     static_assert(P >= kMinP3 && P <= kMaxPR(R) && (P & (P - 1)) == 0, "P must be a supported power of two");
     static constexpr int N = R * P;
     static constexpr int LOGP = ilog2(P);
@@ -67,11 +75,11 @@ struct FftRShape {
     // (Z[k] of FFT ff in region k % R at phys(k / R)); a warp's scatter covers consecutive k
     // of several FFTs.  For R = 3 the offsets past a multiple of 16 are the ones a bank model
     // of that scatter finds best for the block shape of each P (at P = 512: 400 instead of
-    // 768 wavefronts per block); for R = 5 an odd region offset.  The sub-FFT exchanges read
+    // 768 wavefronts per block); for R = 5 and 7 an odd region offset.  The sub-FFT exchanges read
     // and write within one region and are conflict-free for any offset.
     static constexpr int C2R_SUB_EXTRA =
-        R == 5 ? 1 : P == 128 ? 5 : P == 256 ? 1 : P == 512 ? 3 : P == 1024 ? 3 : 11;
-    static constexpr int C2R_FFT_EXTRA = R == 5 ? 0 : P == 128 ? 0 : P == 256 ? 3 : P == 512 ? 3 : P == 1024 ? 15 : 0;
+        R != 3 ? 1 : P == 128 ? 5 : P == 256 ? 1 : P == 512 ? 3 : P == 1024 ? 3 : 11;
+    static constexpr int C2R_FFT_EXTRA = R != 3 ? 0 : P == 128 ? 0 : P == 256 ? 3 : P == 512 ? 3 : P == 1024 ? 15 : 0;
     static constexpr int SUB_C2R = (FftShape<P>::SMEM + 15) / 16 * 16 + C2R_SUB_EXTRA;
     static constexpr int SMEM = R * SUB;               // float2 per exchange buffer
     static constexpr int ROUNDS = (P + T - 1) / T;     // radix-R items per thread
@@ -153,6 +161,20 @@ constexpr float kC51 = 0.309016994374947424102f;  // cos(2 pi / 5)
 constexpr float kC52 = -0.809016994374947424102f; // cos(4 pi / 5)
 constexpr float kS51 = 0.951056516295153572116f;  // sin(2 pi / 5)
 constexpr float kS52 = 0.587785252292473129169f;  // sin(4 pi / 5)
+constexpr float kC71 = 0.623489801858733530525f;  // cos(2 pi / 7)
+constexpr float kC72 = -0.222520933956314404289f; // cos(4 pi / 7)
+constexpr float kC73 = -0.900968867902419126236f; // cos(6 pi / 7)
+constexpr float kS71 = 0.781831482468029808708f;  // sin(2 pi / 7)
+constexpr float kS72 = 0.974927912181823607018f;  // sin(4 pi / 7)
+constexpr float kS73 = 0.433883739117558120475f;  // sin(6 pi / 7)
+
+// cos and sin of 2 pi m / 7, m = 0..6
+__host__ __device__ constexpr float cos7(int m) {
+    return m == 0 ? 1.f : (m == 1 || m == 6) ? kC71 : (m == 2 || m == 5) ? kC72 : kC73;
+}
+__host__ __device__ constexpr float sin7(int m) {
+    return m == 0 ? 0.f : m == 1 ? kS71 : m == 2 ? kS72 : m == 3 ? kS73 : m == 4 ? -kS73 : m == 5 ? -kS72 : -kS71;
+}
 
 // Component k2 of the forward DFT_R of x[0..R-1]: sum_n x[n] W_R^(n k2), W_R = exp(-2 pi i / R).
 template <int R>
@@ -164,6 +186,19 @@ __device__ __forceinline__ float2 dftr_component(const float2 (&x)[R], int k2) {
         const float2 m = make_float2(fmaf(-0.5f, s.x, x[0].x), fmaf(-0.5f, s.y, x[0].y));
         const float hs = k2 == 1 ? -kH3 : kH3;  // -i h d for k2 = 1, +i h d for k2 = 2
         return make_float2(fmaf(-hs, d.y, m.x), fmaf(hs, d.x, m.y));
+    } else if constexpr (R == 7) {
+        // pairs j = 1..3: x_j W^(jk) + x_(7-j) W^(-jk) = c (x_j + x_(7-j)) - i s (x_j - x_(7-j)),
+        // (c, s) = (cos, sin)(2 pi (j k mod 7) / 7)
+        const float2 s1 = cadd(x[1], x[6]), s2 = cadd(x[2], x[5]), s3 = cadd(x[3], x[4]);
+        if (k2 == 0) return cadd(x[0], cadd(s1, cadd(s2, s3)));
+        const float2 d1 = csub(x[1], x[6]), d2 = csub(x[2], x[5]), d3 = csub(x[3], x[4]);
+        const int m1 = k2, m2 = (2 * k2) % 7, m3 = (3 * k2) % 7;
+        const float c1 = cos7(m1), c2 = cos7(m2), c3 = cos7(m3);
+        const float n1 = sin7(m1), n2 = sin7(m2), n3 = sin7(m3);
+        const float2 m = make_float2(fmaf(c3, s3.x, fmaf(c2, s2.x, fmaf(c1, s1.x, x[0].x))),
+                                     fmaf(c3, s3.y, fmaf(c2, s2.y, fmaf(c1, s1.y, x[0].y))));
+        const float2 t = make_float2(fmaf(n3, d3.x, fmaf(n2, d2.x, n1 * d1.x)), fmaf(n3, d3.y, fmaf(n2, d2.y, n1 * d1.y)));
+        return make_float2(m.x + t.y, m.y - t.x);   // m - i t
     } else {
         // X_k = x0 + ca (x1 + x4) + cb (x2 + x3) -+ i [sa (x1 - x4) + sb (x2 - x3)], with
         // (ca, cb, sa, sb) = (c1, c2, s1, s2) for k = 1, 4 and (c2, c1, s2, -s1) for k = 2, 3
@@ -214,6 +249,23 @@ __device__ __forceinline__ void idftr_head(const float2 (&z)[R], int count, Out 
             out(1, make_float2(m.x - hy, m.y + hx));
             if (count > 2) out(2, make_float2(m.x + hy, m.y - hx));
         }
+    } else if constexpr (R == 7) {
+        const float2 s1 = cadd(z[1], z[6]), s2 = cadd(z[2], z[5]), s3 = cadd(z[3], z[4]);
+        out(0, cadd(z[0], cadd(s1, cadd(s2, s3))));
+        const float2 d1 = csub(z[1], z[6]), d2 = csub(z[2], z[5]), d3 = csub(z[3], z[4]);
+        // output n: z0 + sum_j c (z_j + z_(7-j)) + i s (z_j - z_(7-j)), (c, s) at j n mod 7
+#pragma unroll
+        for (int n = 1; n < 7; n++) {
+            if (n < count) {
+                const float c1 = cos7(n), c2 = cos7((2 * n) % 7), c3 = cos7((3 * n) % 7);
+                const float n1 = sin7(n), n2 = sin7((2 * n) % 7), n3 = sin7((3 * n) % 7);
+                const float2 m = make_float2(fmaf(c3, s3.x, fmaf(c2, s2.x, fmaf(c1, s1.x, z[0].x))),
+                                             fmaf(c3, s3.y, fmaf(c2, s2.y, fmaf(c1, s1.y, z[0].y))));
+                const float2 t = make_float2(fmaf(n3, d3.x, fmaf(n2, d2.x, n1 * d1.x)),
+                                             fmaf(n3, d3.y, fmaf(n2, d2.y, n1 * d1.y)));
+                out(n, make_float2(m.x - t.y, m.y + t.x));   // m + i t
+            }
+        }
     } else {
         const float2 s1 = cadd(z[1], z[4]), s2 = cadd(z[2], z[3]);
         out(0, cadd(z[0], cadd(s1, s2)));
@@ -245,6 +297,10 @@ __device__ __forceinline__ void twiddle_powers(float2 (&w)[R], float2 w1) {
     if constexpr (R > 3) {
         w[3] = cmul(w[2], w1);
         w[4] = cmul(w[2], w[2]);
+    }
+    if constexpr (R > 5) {
+        w[5] = cmul(w[4], w1);
+        w[6] = cmul(w[3], w[3]);
     }
 }
 

@@ -1,7 +1,7 @@
-// Launchers for the length-RP pass kernels (kernels_fft3.cuh, R = 3 or 5), templated on R;
-// launch_fft3.cu and launch_fft5.cu each instantiate one radix (separate translation units so
-// the two compile in parallel) and launch_fft3.cu holds the public launchers, which pick the
-// radix of N.  The caller's `tw` is replaced by the two tables these kernels read (sub-FFT
+// Launchers for the length-RP pass kernels (kernels_fft3.cuh, R = 3, 5 or 7), templated on R;
+// launch_fft3.cu, launch_fft5.cu and launch_fft7.cu each instantiate one radix (separate
+// translation units so they compile in parallel) and launch_fft3.cu holds the public
+// launchers, which pick the radix of N.  The caller's `tw` is replaced by the two tables these kernels read (sub-FFT
 // size P, radix-R pass).
 #pragma once
 
@@ -17,7 +17,9 @@ namespace ffb {
         case 128: return FN<R, 128>(__VA_ARGS__);                               \
         case 256: return FN<R, 256>(__VA_ARGS__);                               \
         case 512: return FN<R, 512>(__VA_ARGS__);                               \
-        case 1024: return FN<R, 1024>(__VA_ARGS__);                             \
+        case 1024:                                                              \
+            if constexpr (1024 <= kMaxPR(R)) return FN<R, (R == 7 ? 512 : 1024)>(__VA_ARGS__); \
+            return cudaErrorInvalidValue;                                       \
         case 2048:                                                              \
             if constexpr (2048 <= kMaxPR(R)) return FN<R, (R == 3 ? 2048 : 1024)>(__VA_ARGS__); \
             return cudaErrorInvalidValue;                                       \
@@ -250,7 +252,9 @@ size_t xcorr_smem_r(int n, int img_dtype, int L, int n_batch) {
         case 128: return xcorr3_smem_p<R, 128>(img_dtype, L, n_batch);
         case 256: return xcorr3_smem_p<R, 256>(img_dtype, L, n_batch);
         case 512: return xcorr3_smem_p<R, 512>(img_dtype, L, n_batch);
-        case 1024: return xcorr3_smem_p<R, 1024>(img_dtype, L, n_batch);
+        case 1024:
+            if constexpr (1024 <= kMaxPR(R)) return xcorr3_smem_p<R, (R == 7 ? 512 : 1024)>(img_dtype, L, n_batch);
+            return ~(size_t)0;
         case 2048:
             if constexpr (R == 3) return xcorr3_smem_p<R, 2048>(img_dtype, L, n_batch);
             return ~(size_t)0;
@@ -259,7 +263,8 @@ size_t xcorr_smem_r(int n, int img_dtype, int L, int n_batch) {
 }
 
 
-// The radix-R entry points (explicitly instantiated in launch_fft3.cu and launch_fft5.cu).
+// The radix-R entry points (explicitly instantiated in launch_fft3.cu, launch_fft5.cu and
+// launch_fft7.cu).
 #define FFB_DECLARE_RADIX_LAUNCHERS(EXT, R)                                                       \
     EXT template cudaError_t launch_r2c_r<R>(int, int, const RowFwdArgs&, cudaStream_t);            \
     EXT template cudaError_t launch_c2r_r<R>(int, int, const RowInvArgs&, cudaStream_t);            \

@@ -76,12 +76,14 @@ static __global__ void init_twiddles_r_kernel(float2* tw, int r) {
 __device__ float2 g_twiddles[kTwTotal];
 __device__ float2 g_twiddles3[kTw3Total];
 __device__ float2 g_twiddles5[kTw5Total];
+__device__ float2 g_twiddles7[kTw7Total];
 
 namespace {
 std::mutex g_tw_mutex;
 const float2* g_tw_ptr[64] = {nullptr};
 const float2* g_tw3_ptr[64] = {nullptr};
 const float2* g_tw5_ptr[64] = {nullptr};
+const float2* g_tw7_ptr[64] = {nullptr};
 }  // namespace
 
 cudaError_t twiddles_for(int n, const float2** out) {
@@ -94,11 +96,14 @@ cudaError_t twiddles_for(int n, const float2** out) {
         void* p = nullptr;
         void* p3 = nullptr;
         void* p5 = nullptr;
+        void* p7 = nullptr;
         e = cudaGetSymbolAddress(&p, g_twiddles);
         if (e != cudaSuccess) return e;
         e = cudaGetSymbolAddress(&p3, g_twiddles3);
         if (e != cudaSuccess) return e;
         e = cudaGetSymbolAddress(&p5, g_twiddles5);
+        if (e != cudaSuccess) return e;
+        e = cudaGetSymbolAddress(&p7, g_twiddles7);
         if (e != cudaSuccess) return e;
         cudaStream_t s;
         e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -113,6 +118,10 @@ cudaError_t twiddles_for(int n, const float2** out) {
             init_twiddles_r_kernel<<<(kTw5Total + 255) / 256, 256, 0, s>>>(static_cast<float2*>(p5), 5);
             e = cudaGetLastError();
         }
+        if (e == cudaSuccess) {
+            init_twiddles_r_kernel<<<(kTw7Total + 255) / 256, 256, 0, s>>>(static_cast<float2*>(p7), 7);
+            e = cudaGetLastError();
+        }
         cudaError_t e2 = cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
         if (e != cudaSuccess) return e;
@@ -120,6 +129,7 @@ cudaError_t twiddles_for(int n, const float2** out) {
         g_tw_ptr[dev] = static_cast<const float2*>(p);
         g_tw3_ptr[dev] = static_cast<const float2*>(p3);
         g_tw5_ptr[dev] = static_cast<const float2*>(p5);
+        g_tw7_ptr[dev] = static_cast<const float2*>(p7);
     }
     if (is_3p_size(n)) {
         *out = g_tw3_ptr[dev] + twr_base(3, n / 3);
@@ -127,6 +137,10 @@ cudaError_t twiddles_for(int n, const float2** out) {
     }
     if (is_5p_size(n)) {
         *out = g_tw5_ptr[dev] + twr_base(5, n / 5);
+        return cudaSuccess;
+    }
+    if (is_7p_size(n)) {
+        *out = g_tw7_ptr[dev] + twr_base(7, n / 7);
         return cudaSuccess;
     }
     if (!is_pow2_size(n) || n < kMinN || n > kMaxN) return cudaErrorInvalidValue;

@@ -67,7 +67,9 @@ def test_memory_sizes_match_reference(fin, fout, iout):
     ((64, 64, 1), (320, 320, 1), (320, 320, 1), (320, 320, 1), C.ERR_INVALID_DIMS),  # 5 * 2^k below 640
     ((64, 64, 1), (10240, 64, 1), (10240, 64, 1), (10240, 64, 1), C.ERR_INVALID_DIMS),  # 5 * 2^k above 5120
     ((16, 16, 16), (320, 320, 320), (320, 320, 320), (320, 320, 320), C.ERR_INVALID_DIMS),  # 5 * 2^k in 3D
-    ((64, 64, 1), (448, 448, 1), (448, 448, 1), (448, 448, 1), C.ERR_INVALID_DIMS),  # 7 * 2^k
+    ((64, 64, 1), (448, 448, 1), (448, 448, 1), (448, 448, 1), C.ERR_INVALID_DIMS),  # 7 * 2^k below 896
+    ((64, 64, 1), (7168, 64, 1), (7168, 64, 1), (7168, 64, 1), C.ERR_INVALID_DIMS),  # 7 * 2^k above 3584
+    ((16, 16, 16), (448, 448, 448), (448, 448, 448), (448, 448, 448), C.ERR_INVALID_DIMS),  # 7 * 2^k in 3D
     ((64, 64, 1), (192, 192, 1), (192, 192, 1), (192, 192, 1), C.ERR_INVALID_DIMS),  # 3 * 2^k below 384
     ((16, 16, 16), (384, 384, 384), (384, 384, 384), (384, 384, 384), C.ERR_INVALID_DIMS),  # 3 * 2^k in 3D
     ((64, 64, 1), (512, 512, 1), (512, 512, 1), (600, 600, 1), C.ERR_INVALID_DIMS),  # inverse grows, non-pow2
@@ -91,6 +93,8 @@ def test_validation_rejects(fin, fout, iin, iout, status):
     ((64, 64, 1), (640, 640, 1), (640, 640, 1)),
     ((100, 200, 1), (1280, 5120, 1), (1280, 5120, 1)),
     ((1000, 10, 1), (2560, 32, 1), (2000, 20, 1)),
+    ((64, 64, 1), (896, 896, 1), (896, 896, 1)),
+    ((100, 200, 1), (1792, 3584, 1), (1792, 3584, 1)),
 ])
 def test_three_times_power_of_two_lengths_accepted_in_2d(fin, fout, iout):
     ft = new()

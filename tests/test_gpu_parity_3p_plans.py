@@ -1,4 +1,4 @@
-"""2D plans at the lengths 3 * 2^k (384 ... 6144) and 5 * 2^k (640 ... 5120), which the
+"""2D plans at the lengths 3 * 2^k (384 ... 6144), 5 * 2^k (640 ... 5120) and 7 * 2^k (896 ... 3584), which the
 reference rejects, against the FP64 oracle: forward, inverse (with a window origin), round
 trip, and the fused correlation through the size-N kernels (single call) and the
 reduced-size path (batched).
@@ -34,6 +34,12 @@ FWD_CASES = [
     ((32, 5120, 1), (32, 5120, 1)),           # 5120-point columns
     ((640, 1536, 1), (640, 1536, 1)),         # 5 * 2^k rows, 3 * 2^k columns
     ((2560, 1280, 1), (640, 640, 1)),         # forward decrease
+    ((896, 896, 1), (896, 896, 1)),           # 7 * 2^k
+    ((100, 300, 1), (896, 1792, 1)),          # zero padding into 7 * 2^k on both axes
+    ((3584, 32, 1), (3584, 32, 1)),           # 3584-point rows
+    ((32, 3584, 1), (32, 3584, 1)),           # 3584-point columns
+    ((896, 1536, 1), (896, 1536, 1)),         # 7 * 2^k rows, 3 * 2^k columns
+    ((1792, 896, 1), (640, 640, 1)),          # forward decrease
 ]
 
 
@@ -58,6 +64,8 @@ INV_CASES = [
     ((1280, 1280, 1), (1280, 1280, 1), (0, 0)),
     ((640, 2560, 1), (600, 2000, 1), (0, 0)),
     ((2560, 640, 1), (1000, 500, 1), (40, 70)),
+    ((1792, 1792, 1), (1792, 1792, 1), (0, 0)),
+    ((896, 3584, 1), (800, 3000, 1), (20, 30)),
 ]
 
 

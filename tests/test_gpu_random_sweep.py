@@ -1,6 +1,6 @@
 """Seeded random sweep of plan shapes and functors against the FP64 oracle.
 
-Each case draws a transform length per axis among powers of two, 3 * 2^k and 5 * 2^k, a
+Each case draws a transform length per axis among powers of two, 3 * 2^k, 5 * 2^k and 7 * 2^k, a
 template (forward input) no larger than the transform, a window (inverse output) no larger
 than it, functors among NOOP / SCALE / CONJ_MUL / CONJ_MUL_THEN_SCALE, and runs the
 correlation through the single call (size-N kernels), the batched call (reduced size where
@@ -16,7 +16,7 @@ from tests._util import RTOL_L2_FP32, dev, empty, host, spectrum_view
 
 pytestmark = pytest.mark.gpu
 
-LENGTHS = [64, 128, 256, 384, 512, 640, 768, 1024, 1280]
+LENGTHS = [64, 128, 256, 384, 512, 640, 768, 896, 1024, 1280, 1792]
 
 
 def draw(seed):

@@ -1,8 +1,9 @@
-"""Batched correlation at the mixed-radix lengths 3 * 2^k and 5 * 2^k against the FP64 oracle.
+"""Batched correlation at the mixed-radix lengths 3 * 2^k, 5 * 2^k and 7 * 2^k against the FP64 oracle.
 
-When 3 * 2^k (2^k in [128, 2048]) or 5 * 2^k (2^k in [128, 1024]) reaches L + W - 1 before
-the next power of two, the batched call correlates at that length (three or five radix-16
-sub-FFTs and a radix-3 or radix-5 pass per transform).  These tests drive every such length along each axis through all four
+When 3 * 2^k (2^k in [128, 2048]) or 5 * 2^k (2^k in [128, 1024]) reaches L + W - 1 before the
+next power of two, the batched call correlates at that length (R radix-16 sub-FFTs and a
+radix-R pass per transform); 7 * 2^k lengths (2^k in [128, 512]) are used where the plan's
+own N is one.  These tests drive every such length along each axis through all four
 kernels that have a 3 * 2^k form (row R2C, fused column pass, row C2R, and the forward
 column pass of the image preparation) and compare the retained windows with the size-N
 correlation that the reference defines.
@@ -59,7 +60,15 @@ CASES5 = [
 ]
 
 
-@pytest.mark.parametrize("fin,fout,iout,msize", CASES3 + CASES5)
+CASES7 = [
+    ((100, 100, 1), (896, 896, 1), (751, 751, 1), (896, 896)),          # plan at 7 * 128 (850 needs all of it)
+    ((300, 300, 1), (1792, 1792, 1), (1401, 1401, 1), (1792, 1792)),    # plan at 7 * 256
+    ((1000, 16, 1), (3584, 64, 1), (2301, 16, 1), (3584, 32)),          # 7 * 512 rows, reduced along y
+    ((16, 1000, 1), (64, 3584, 1), (16, 2301, 1), (32, 3584)),          # 7 * 512 fused column pass
+]
+
+
+@pytest.mark.parametrize("fin,fout,iout,msize", CASES3 + CASES5 + CASES7)
 def test_mixed_radix_sizes_match_oracle(torch_cuda, fin, fout, iout, msize):
     torch = torch_cuda
     ft = plan(fin, fout, iout)
