@@ -58,6 +58,15 @@ static inline int xcorr_tpb(const fastfft_plan_s* h, int n, long long my) {
 #ifndef FFB_ENABLE_FFT3
 #define FFB_ENABLE_FFT3 1
 #endif
+// Lengths 5 * 2^k among the reduced-size correlation's lengths (1), or not (0, the default):
+// measured on B200 (64 templates per call) the 3 * 2^k length above a 5 * 2^k one is as fast or
+// faster although 6/5 as long: 264,767 at 768 against 246,111 templates/s at 640 (128^2
+// templates, 512^2 windows), 96,051 at 1536 against 89,653 at 1280 (300^2, 900^2), 23,681 at
+// 3072 against 23,809 at 2560 (700^2, 1800^2); the uneven 1024-template batch gains 3.5 %.
+// 5 * 2^k lengths run where a plan's own N is one.
+#ifndef FFB_ENABLE_FFT5
+#define FFB_ENABLE_FFT5 0
+#endif
 // Lengths 7 * 2^k among the reduced-size correlation's lengths (1), or not (0, the default):
 // a 7 * 2^k transform costs far more per point than the power of two above it (measured on
 // B200 in the uneven 1024-template batch, whose 384^2 templates with 512^2 windows would
@@ -187,15 +196,17 @@ long long pow2_at_least(long long v) {
 }
 
 // Smallest transform length >= v of the reduced-size correlation: a power of two, or
-// 3 * 2^k (kMinP3 <= 2^k <= kMaxP3) or 5 * 2^k (kMinP3 <= 2^k <= kMaxP5) when shorter (and
-// 7 * 2^k with FFB_ENABLE_FFT7).
+// 3 * 2^k (kMinP3 <= 2^k <= kMaxP3) when shorter (and 5 * 2^k, 7 * 2^k with FFB_ENABLE_FFT5,
+// FFB_ENABLE_FFT7).
 long long corr_size_at_least(long long v) {
     long long best = std::max<long long>(ffb::kMinN, pow2_at_least(v));
 #if FFB_ENABLE_FFT3
     for (long long p = ffb::kMinP3; p <= ffb::kMaxP3; p *= 2)
         if (3 * p >= v && 3 * p < best) best = 3 * p;
+#if FFB_ENABLE_FFT5
     for (long long p = ffb::kMinP3; p <= ffb::kMaxP5; p *= 2)
         if (5 * p >= v && 5 * p < best) best = 5 * p;
+#endif
 #if FFB_ENABLE_FFT7
     for (long long p = ffb::kMinP3; p <= ffb::kMaxP7; p *= 2)
         if (7 * p >= v && 7 * p < best) best = 7 * p;

@@ -208,8 +208,8 @@ FASTFFT_API fastfft_status fastfft_templates_per_block(fastfft_handle h, int* n)
 FASTFFT_API fastfft_status fastfft_set_pipelined_groups(fastfft_handle h, int n);
 FASTFFT_API fastfft_status fastfft_pipelined_groups(fastfft_handle h, int* n);
 
-/* The batched call correlates at the smallest supported size M >= L + W - 1 per axis (a
- * power of two, 3 * 2^k or 5 * 2^k) when that is below the plan's N (template in [0, L),
+/* The batched call correlates at the smallest size M >= L + W - 1 per axis among powers of
+ * two and 3 * 2^k when that is below the plan's N (template in [0, L),
  * window in [0, W)): every retained lag then reads image pixels in [0, L + W - 1) only, so
  * the size-M circular correlation against the spectrum of the image cropped to [0, M) gives
  * the same values as the size-N one.  This holds for the correlation intra-ops (CONJ_MUL,

@@ -162,3 +162,27 @@ def test_tall_templates_fall_back_to_fp32(torch_cuda):
     ft = _plan((64, 520, 1), (2048, 2048, 1), (64, 1000, 1), True)
     assert ft.CorrelationSize()[1] == 1536
     assert not ft.TensorCoreDFTActive()
+
+
+@pytest.mark.parametrize("per_launch,groups", [(3, 2), (5, 1), (16, 2)])
+def test_several_launches_and_groups_in_flight(torch_cuda, per_launch, groups):
+    """The tensor-core pass with several launches per call and two groups in flight on two
+    streams (each launch takes whole SMs and all of their tensor memory while it runs):
+    windows identical to one launch of the same pass."""
+    torch = torch_cuda
+    img, spec, d_spec = _blob_case(torch, 55)
+    rng = np.random.default_rng(56)
+    ts = [rng.standard_normal((384, 384)).astype(np.float32) for _ in range(11)]
+    d_ts = [dev(torch, O.real_to_padded(t, HEAD_FIN)) for t in ts]
+    results = []
+    for pl, gr in ((64, 1), (per_launch, groups)):
+        ft = _plan(HEAD_FIN, HEAD_FOUT, HEAD_IOUT, True)
+        ft.SetTemplatesPerLaunch(pl)
+        ft.SetPipelinedGroups(gr)
+        assert ft.TensorCoreDFTActive()
+        outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+        ft.FwdImageInvFFTMany(d_ts, d_spec, outs)
+        torch.cuda.synchronize()
+        results.append([host(o) for o in outs])
+    for a, b in zip(*results):
+        assert np.array_equal(a, b)

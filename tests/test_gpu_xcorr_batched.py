@@ -29,7 +29,7 @@ def image_spectrum(fout, seed):
 CASES = [
     ((48, 48, 1), (512, 512, 1), (40, 40, 1), (128, 128)),
     ((100, 60, 1), (1024, 512, 1), (130, 70, 1), (256, 256)),
-    ((128, 128, 1), (4096, 4096, 1), (512, 512, 1), (640, 640)),     # 639 -> 5 * 128
+    ((128, 128, 1), (4096, 4096, 1), (512, 512, 1), (768, 768)),     # 639 -> 3 * 256
     ((256, 256, 1), (1024, 1024, 1), (512, 512, 1), (768, 768)),
     ((256, 256, 1), (512, 512, 1), (300, 300, 1), (512, 512)),       # 555 > 512: full size
     ((33, 200, 1), (64, 2048, 1), (30, 100, 1), (64, 384)),
@@ -222,8 +222,8 @@ def test_launches_beyond_sixteen_templates(torch_cuda):
 
 
 def test_uneven_templates_use_their_own_size_class(torch_cuda):
-    """128^2 and 384^2 templates with 512^2 windows in one call: the 128s correlate at 640
-    (128 + 511 <= 5 * 128), the 384s at the plan's 1024; one image preparation per class."""
+    """128^2 and 384^2 templates with 512^2 windows in one call: the 128s correlate at 768
+    (128 + 511 <= 3 * 256), the 384s at the plan's 1024; one image preparation per class."""
     torch = torch_cuda
     fmax, fout, iout = (384, 384, 1), (2048, 2048, 1), (512, 512, 1)
     ft = plan(fmax, fout, iout)
@@ -290,10 +290,11 @@ def test_pipelined_groups_match_single_stream(torch_cuda, per_launch):
 
 def test_templates_per_block_setting(torch_cuda):
     """Every templates-per-block choice of the fused column pass gives bit-identical windows
-    (only the grouping of templates into blocks changes), at 1536 and at 640 points."""
+    (only the grouping of templates into blocks changes), at 1536 and at 640 points (a plan whose
+    columns are 640 long, reduced along x only)."""
     torch = torch_cuda
     for fin, fout, iout in (((384, 384, 1), (2048, 2048, 1), (1024, 1024, 1)),
-                            ((128, 128, 1), (1024, 1024, 1), (512, 512, 1))):
+                            ((16, 128, 1), (64, 640, 1), (16, 512, 1))):
         spec = dev(torch, image_spectrum(fout, 27).view(np.float32))
         rng = np.random.default_rng(28)
         ins = [dev(torch, O.real_to_padded(rng.standard_normal((fin[1], fin[0])).astype(np.float32), fin))

@@ -1,9 +1,9 @@
 """Batched correlation at the mixed-radix lengths 3 * 2^k, 5 * 2^k and 7 * 2^k against the FP64 oracle.
 
-When 3 * 2^k (2^k in [128, 2048]) or 5 * 2^k (2^k in [128, 1024]) reaches L + W - 1 before the
-next power of two, the batched call correlates at that length (R radix-16 sub-FFTs and a
-radix-R pass per transform); 7 * 2^k lengths (2^k in [128, 512]) are used where the plan's
-own N is one.  These tests drive every such length along each axis through all four
+When 3 * 2^k (2^k in [128, 2048]) reaches L + W - 1 before the next power of two, the batched
+call correlates at that length (R radix-16 sub-FFTs and a radix-R pass per transform); 5 * 2^k
+(2^k in [128, 1024]) and 7 * 2^k (2^k in [128, 512]) lengths run where the plan's own N is one
+(along an axis without reduction, or with the other axis reduced).  These tests drive every such length along each axis through all four
 kernels that have a 3 * 2^k form (row R2C, fused column pass, row C2R, and the forward
 column pass of the image preparation) and compare the retained windows with the size-N
 correlation that the reference defines.
@@ -49,14 +49,14 @@ CASES3 = [
 
 
 CASES5 = [
-    ((128, 128, 1), (1024, 1024, 1), (512, 512, 1), (640, 640)),        # 639 -> 5 * 128
-    ((300, 300, 1), (2048, 2048, 1), (900, 900, 1), (1280, 1280)),      # 1199 -> 5 * 256
-    ((300, 200, 1), (2048, 1024, 1), (500, 600, 1), (1024, 1024)),      # 799 -> 1024, 799 -> 1024 (x), 5 * 2^k only where shorter
-    ((1000, 16, 1), (4096, 64, 1), (1500, 16, 1), (2560, 32)),          # 2499 -> 5 * 512 along x
-    ((16, 1000, 1), (64, 4096, 1), (16, 1500, 1), (32, 2560)),          # ... along y
-    ((2000, 8, 1), (8192, 32, 1), (3000, 8, 1), (5120, 16)),            # 4999 -> 5 * 1024 along x
-    ((8, 2000, 1), (32, 8192, 1), (8, 3000, 1), (16, 5120)),            # ... along y
-    ((200, 150, 1), (1024, 1024, 1), (440, 600, 1), (640, 768)),        # 639 -> 5 * 128, 749 -> 3 * 256
+    ((128, 128, 1), (640, 640, 1), (512, 512, 1), (640, 640)),          # plan at 5 * 128 (639 needs all of it)
+    ((300, 300, 1), (1280, 1280, 1), (900, 900, 1), (1280, 1280)),      # plan at 5 * 256
+    ((300, 200, 1), (2048, 1024, 1), (500, 600, 1), (1024, 1024)),      # 799 -> 1024 on both axes
+    ((1000, 16, 1), (2560, 64, 1), (1500, 16, 1), (2560, 32)),          # 5 * 512 rows, reduced along y
+    ((16, 1000, 1), (64, 2560, 1), (16, 1500, 1), (32, 2560)),          # 5 * 512 fused column pass
+    ((2000, 8, 1), (5120, 32, 1), (3000, 8, 1), (5120, 16)),            # 5 * 1024 rows
+    ((8, 2000, 1), (32, 5120, 1), (8, 3000, 1), (16, 5120)),            # 5 * 1024 fused column pass
+    ((200, 150, 1), (1024, 1024, 1), (440, 600, 1), (768, 768)),        # 639, 749 -> 3 * 256
 ]
 
 
