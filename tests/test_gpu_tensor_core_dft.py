@@ -186,3 +186,24 @@ def test_several_launches_and_groups_in_flight(torch_cuda, per_launch, groups):
         results.append([host(o) for o in outs])
     for a, b in zip(*results):
         assert np.array_equal(a, b)
+
+
+def test_longest_template_and_widest_window(torch_cuda):
+    """The pass's limits: 512-row templates (F1 reads n1 < 16 of 32-row steps) and a 1025-row
+    window (the inverse keeps n1 < 48, N = 96 of the last product), L + W - 1 = 1536 exactly."""
+    torch = torch_cuda
+    fin, fout, iout = (64, 512, 1), (2048, 2048, 1), (300, 1025, 1)
+    ft = _plan(fin, fout, iout, True)
+    assert ft.CorrelationSize()[1] == 1536 and ft.TensorCoreDFTActive()
+    img = O.gaussian_blob_image(2048, n_blobs=8, seed=57)
+    spec = O.image_spectrum_fp32(img)
+    d_spec = dev(torch, spec.view(np.float32))
+    rng = np.random.default_rng(58)
+    ts = [rng.standard_normal((fin[1], fin[0])).astype(np.float32) for _ in range(5)]
+    outs = [empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32) for _ in ts]
+    ft.FwdImageInvFFTMany([dev(torch, O.real_to_padded(t, fin)) for t in ts], d_spec, outs)
+    torch.cuda.synchronize()
+    p = O.Plan(fin, fout, fout, iout)
+    for t, o in zip(ts, outs):
+        ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), spec, p, out_dtype=np.float64), iout)
+        assert O.rel_l2(O.real_from_padded(host(o), iout), ref) <= RTOL_L2_TC
