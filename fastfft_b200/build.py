@@ -16,7 +16,7 @@ CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "libfastfft_b200.so"
 SOURCES = ["launch_fft7.cu", "launch_fft5.cu", "launch_fft3.cu", "twiddles.cu", "launch_rows.cu", "launch_cols.cu", "launch_xcorr.cu",
-           "capi.cu", "noalloc.cu", "spectrum_ops.cu", "launch_tc.cu"]
+           "capi.cu", "noalloc.cu", "spectrum_ops.cu", "launch_tc.cu", "launch_blue.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",

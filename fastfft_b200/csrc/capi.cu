@@ -159,12 +159,15 @@ fastfft_status validate(fastfft_plan_s* h) {
     if (dim != h->rank) return fail(h, FASTFFT_ERR_INVALID_DIMS, "plan dimensionality does not match the handle rank");
     // transform lengths: powers of two (FastFFT.cu:895-927); real-input 2D plans also take
     // 3 * 2^k with 128 <= 2^k <= 2048 (384 ... 6144), 5 * 2^k with 128 <= 2^k <= 1024
-    // (640 ... 5120) and 7 * 2^k with 128 <= 2^k <= 512 (896 ... 3584), which the reference
-    // rejects
+    // (640 ... 5120) and 7 * 2^k with 128 <= 2^k <= 512 (896 ... 3584), and any other length
+    // in [17, 4096] (chirp-z on a power-of-two FFT), which the reference rejects
     const bool wide = dim == 2 && !cplx_dtype(h->input_dtype);
-    auto len_ok = [&](long long v) { return is_pow2(v) || (wide && v <= 6144 && ffb::is_rp_size((int)v)); };
-    const char* lens =
-        wide ? "powers of 2, 3 * 2^k (384 ... 6144), 5 * 2^k (640 ... 5120) or 7 * 2^k (896 ... 3584)" : "powers of 2";
+    auto len_ok = [&](long long v) {
+        return is_pow2(v) || (wide && v <= 6144 && (ffb::is_rp_size((int)v) || ffb::is_blue_size((int)v)));
+    };
+    const char* lens = wide ? "powers of 2, 3 * 2^k (384 ... 6144), 5 * 2^k (640 ... 5120), 7 * 2^k (896 ... 3584) "
+                              "or any length in [17, 4096]"
+                            : "powers of 2";
     if ((!len_ok(fi.x) || !len_ok(fi.y) || !is_pow2(fi.z)) && h->fwd_change != SizeChange::Increase)
         return fail(h, FASTFFT_ERR_INVALID_DIMS,
                     std::string("input dimensions must be ") + lens + " unless the forward transform pads");
@@ -246,7 +249,9 @@ void size_buffers(fastfft_plan_s* h) {
         const long long nx = h->fwd_out.x, ny = h->fwd_out.y;
         const long long mx = std::min(nx, corr_size_at_least(h->fwd_in.x + h->inv_out.x - 1));
         const long long my = std::min(ny, corr_size_at_least(h->fwd_in.y + h->inv_out.y - 1));
-        if (mx < nx || my < ny) {
+        // (an axis whose correlation would run at the plan's own chirp-z length keeps the
+        // whole call at the plan's size: the batched kernels run powers of two and R * 2^k)
+        if ((mx < nx || my < ny) && !ffb::is_blue_size((int)mx) && !ffb::is_blue_size((int)my)) {
             h->red_ok = true;
             h->red_mx = mx;
             h->red_my = my;
@@ -1161,6 +1166,9 @@ static fastfft_status xcorr_many(fastfft_handle h, int n, const void* const* inp
         if (e != cudaSuccess) return cuda_fail(h, e, "clearing the peak array");
     }
     if (!h->red_ok || h->force_full_size || !correlation_op(intra_op)) {
+        if ((peaks || mip) && ffb::is_blue_size((int)h->inv_in.x))
+            return fail(h, FASTFFT_ERR_UNSUPPORTED,
+                        "the fused peak search and projection need a power-of-two or R * 2^k inverse row length");
         for (int i = 0; i < n; i++) {
             void* out = reduce ? (outputs ? outputs[i] : nullptr)
                                : ((outputs && outputs[i]) ? outputs[i] : const_cast<void*>(inputs[i]));

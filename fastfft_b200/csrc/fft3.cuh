@@ -44,6 +44,17 @@ __host__ __device__ constexpr bool is_7p_size(int n) {
     return n > 0 && n % 7 == 0 && is_pow2_size(n / 7) && n / 7 >= kMinP3 && n / 7 <= kMaxP7;
 }
 __host__ __device__ constexpr bool is_rp_size(int n) { return is_3p_size(n) || is_5p_size(n) || is_7p_size(n); }
+// Lengths of the chirp-z (Bluestein) path (kernels_blue.cuh): any other length in [17, 4096],
+// on the power-of-two block FFT of length blue_m(n) >= 2n - 1.
+constexpr int kMaxBlueN = 4096;
+__host__ __device__ constexpr bool is_blue_size(int n) {
+    return n >= 17 && n <= kMaxBlueN && !is_pow2_size(n) && !is_rp_size(n);
+}
+__host__ __device__ constexpr int blue_m(int n) {
+    int m = 64;
+    while (m < 2 * n - 1) m *= 2;
+    return m;
+}
 // the radix R of a length R * 2^k (1 for a power of two)
 __host__ __device__ constexpr int radix_of(int n) {
     return is_3p_size(n) ? 3 : is_5p_size(n) ? 5 : is_7p_size(n) ? 7 : 1;

@@ -64,14 +64,17 @@ static cudaError_t xcorr_dispatch(int img_dtype, const ColArgs& a, cudaStream_t 
 
 cudaError_t launch_cols_fwd(int n, int out_dtype, const ColArgs& a, cudaStream_t st) {
     if (is_rp_size(n)) return launch_cols3_fwd(n, out_dtype, a, st);
+    if (is_blue_size(n)) return launch_blue_cols(n, COL_FWD, out_dtype, a, st);
     FFB_SIZE_SWITCH(n, fwd_dispatch, out_dtype, a, st)
 }
 cudaError_t launch_cols_inv(int n, int in_dtype, const ColArgs& a, cudaStream_t st) {
     if (is_rp_size(n)) return launch_cols3_inv(n, in_dtype, a, st);
+    if (is_blue_size(n)) return launch_blue_cols(n, COL_INV, in_dtype, a, st);
     FFB_SIZE_SWITCH(n, inv_dispatch, in_dtype, a, st)
 }
 cudaError_t launch_cols_xcorr(int n, int img_dtype, const ColArgs& a, cudaStream_t st) {
     if (is_rp_size(n)) return launch_cols3_xcorr(n, img_dtype, a, st);
+    if (is_blue_size(n)) return launch_blue_cols(n, COL_XCORR, img_dtype, a, st);
     FFB_SIZE_SWITCH(n, xcorr_dispatch, img_dtype, a, st)
 }
 

@@ -32,6 +32,7 @@ static cudaError_t r2c_dispatch(int in_dtype, const RowFwdArgs& a, cudaStream_t 
 
 cudaError_t launch_r2c_rows(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st) {
     if (is_rp_size(n)) return launch_r2c3(n, in_dtype, a, st);
+    if (is_blue_size(n)) return launch_blue_r2c(n, in_dtype, a, st);
     FFB_SIZE_SWITCH(n, r2c_dispatch, in_dtype, a, st)
 }
 
@@ -63,6 +64,7 @@ static cudaError_t c2r_dispatch(int out_dtype, const RowInvArgs& a, cudaStream_t
 
 cudaError_t launch_c2r_rows(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st) {
     if (is_rp_size(n)) return launch_c2r3(n, out_dtype, a, st);
+    if (is_blue_size(n)) return launch_blue_c2r(n, out_dtype, a, st);
     FFB_SIZE_SWITCH(n, c2r_dispatch, out_dtype, a, st)
 }
 

@@ -143,6 +143,7 @@ cudaError_t twiddles_for(int n, const float2** out) {
         *out = g_tw7_ptr[dev] + twr_base(7, n / 7);
         return cudaSuccess;
     }
+    if (is_blue_size(n)) n = blue_m(n);   // the chirp-z path runs on the power-of-two FFT of this length
     if (!is_pow2_size(n) || n < kMinN || n > kMaxN) return cudaErrorInvalidValue;
     int base = 0;
     for (int m = kMinN; m < n; m *= 2) base += tw_size_of(m);

@@ -63,16 +63,16 @@ def test_memory_sizes_match_reference(fin, fout, iout):
 @pytest.mark.parametrize("fin,fout,iin,iout,status", [
     ((64, 64, 1), (512, 512, 1), (256, 256, 1), (256, 256, 1), C.ERR_INVALID_DIMS),  # fwd out != inv in
     ((64, 128, 1), (128, 64, 1), (128, 64, 1), (128, 64, 1), C.ERR_INVALID_DIMS),    # mixed grow/shrink
-    ((100, 100, 1), (100, 100, 1), (100, 100, 1), (100, 100, 1), C.ERR_INVALID_DIMS),  # non-pow2, no pad
-    ((64, 64, 1), (320, 320, 1), (320, 320, 1), (320, 320, 1), C.ERR_INVALID_DIMS),  # 5 * 2^k below 640
     ((64, 64, 1), (10240, 64, 1), (10240, 64, 1), (10240, 64, 1), C.ERR_INVALID_DIMS),  # 5 * 2^k above 5120
     ((16, 16, 16), (320, 320, 320), (320, 320, 320), (320, 320, 320), C.ERR_INVALID_DIMS),  # 5 * 2^k in 3D
-    ((64, 64, 1), (448, 448, 1), (448, 448, 1), (448, 448, 1), C.ERR_INVALID_DIMS),  # 7 * 2^k below 896
     ((64, 64, 1), (7168, 64, 1), (7168, 64, 1), (7168, 64, 1), C.ERR_INVALID_DIMS),  # 7 * 2^k above 3584
     ((16, 16, 16), (448, 448, 448), (448, 448, 448), (448, 448, 448), C.ERR_INVALID_DIMS),  # 7 * 2^k in 3D
-    ((64, 64, 1), (192, 192, 1), (192, 192, 1), (192, 192, 1), C.ERR_INVALID_DIMS),  # 3 * 2^k below 384
     ((16, 16, 16), (384, 384, 384), (384, 384, 384), (384, 384, 384), C.ERR_INVALID_DIMS),  # 3 * 2^k in 3D
-    ((64, 64, 1), (512, 512, 1), (512, 512, 1), (600, 600, 1), C.ERR_INVALID_DIMS),  # inverse grows, non-pow2
+    ((64, 64, 1), (5000, 64, 1), (5000, 64, 1), (5000, 64, 1), C.ERR_INVALID_DIMS),  # other length above 4096
+    ((64, 64, 1), (4097, 4097, 1), (4097, 4097, 1), (4097, 4097, 1), C.ERR_INVALID_DIMS),
+    ((8, 8, 1), (12, 12, 1), (12, 12, 1), (12, 12, 1), C.ERR_INVALID_DIMS),  # other length below 17
+    ((16, 16, 16), (100, 100, 100), (100, 100, 100), (100, 100, 100), C.ERR_INVALID_DIMS),  # other length in 3D
+    ((64, 64, 1), (512, 512, 1), (512, 512, 1), (5000, 5000, 1), C.ERR_INVALID_DIMS),  # inverse grows, bad length
     ((64, 64, 64), (1024, 1024, 1024), (1024, 1024, 1024), (1024, 1024, 1024), C.ERR_INVALID_DIMS),  # 3D > 512
     ((64, 64, 1), (16384, 16384, 1), (16384, 16384, 1), (16384, 16384, 1), C.ERR_UNSUPPORTED),  # > 8192
     ((4, 4, 1), (8, 8, 1), (8, 8, 1), (8, 8, 1), C.ERR_UNSUPPORTED),  # < 16
@@ -95,6 +95,12 @@ def test_validation_rejects(fin, fout, iin, iout, status):
     ((1000, 10, 1), (2560, 32, 1), (2000, 20, 1)),
     ((64, 64, 1), (896, 896, 1), (896, 896, 1)),
     ((100, 200, 1), (1792, 3584, 1), (1792, 3584, 1)),
+    # any other length in [17, 4096] (chirp-z transforms)
+    ((100, 100, 1), (100, 100, 1), (100, 100, 1)),
+    ((64, 64, 1), (320, 448, 1), (320, 448, 1)),
+    ((64, 64, 1), (192, 192, 1), (192, 192, 1)),
+    ((77, 53, 1), (999, 1001, 1), (700, 600, 1)),
+    ((17, 4095, 1), (17, 4095, 1), (17, 4095, 1)),
 ])
 def test_three_times_power_of_two_lengths_accepted_in_2d(fin, fout, iout):
     ft = new()
