@@ -24,7 +24,8 @@ ranks.  --impl reference times the host CPU implementation of the same transform
 restatement in oracle/, multithreaded pocketfft) on rank 0.
 
 Besides the headline line's own keys, the JSON line carries the other workload families
-(64^2 -> 512^2 round trip; 64^3 -> 256^3 forward with the central 128^3 inverse; the
+(64^2 -> 512^2 round trip; a 1000^2 round trip on the chirp-z path beside 1024^2;
+64^3 -> 256^3 forward with the central 128^3 inverse; the
 uneven 1024-template batch; FP16/BF16 storage with and without the tensor-core DFT) and
 the cuFFT comparators (full size and the same reduced size), each with its accuracy
 against the FP64 oracle.
@@ -557,6 +558,70 @@ def run_round_trip_2d(dev, local, min_seconds):
                          "round_trip_rel_max_vs_fp64": O.rel_max(back_got, back_ref)}}
 
 
+def run_any_length_2d(dev, local, min_seconds):
+    """Plans at a length that is neither a power of two nor R * 2^k (chirp-z transforms):
+    N(0,1) 1000^2 R2C (FwdFFT) then C2R (InvFFT), batch 1, beside the same round trip at
+    1024^2 (the power-of-two passes).  12 buffer sets rotate (> 126 MB L2); the round trips
+    replay from a CUDA graph."""
+    import torch
+
+    import fastfft_b200 as F
+    from oracle import fastfft_oracle as O
+
+    sets = 12
+    peak, _ = measured_hbm_peak()
+    res = {"workload": "2D FP32 R2C n^2 -> n^2 then C2R n^2 -> n^2, batch 1, n = 1000 (chirp-z on 2048-point "
+                       "FFTs) and n = 1024", "unit": "round trips/s"}
+    for n in (1000, 1024):
+        dims = (n, n, 1)
+        ft = F.FourierTransformer()
+        ft.SetForwardFFTPlan(*dims, *dims)
+        ft.SetInverseFFTPlan(*dims, *dims)
+        rng = np.random.default_rng(O.SEED_BASE + n)
+        x = rng.standard_normal((n, n)).astype(np.float32)
+        xin = torch.from_numpy(O.real_to_padded(x, dims)).to(dev)
+        ins = [xin.clone() for _ in range(sets)]
+        specs = [torch.empty(ft.ReturnFwdOutputMemorySize(), device=dev) for _ in range(sets)]
+        outs = [torch.empty(ft.ReturnInvOutputMemorySize(), device=dev) for _ in range(sets)]
+
+        def all_sets():
+            for i in range(sets):
+                ft.FwdFFT(ins[i], specs[i])
+                ft.InvFFT(specs[i], outs[i])
+
+        all_sets()
+        all_sets()
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            all_sets()
+        graph.replay()
+        reps = reps_for(torch, graph.replay, min_seconds / 2)
+        clocks = ClockSampler(smi_index(local))
+        clocks.start()
+        ms = event_ms(torch, graph.replay, reps) / (reps * sets)
+        clk = clocks.stop()
+        del graph
+        w, pitch = O.padded_x(n)
+        byts = 2 * (n * pitch * 4 + w * n * 8)     # real in + spectrum out, spectrum in + real out
+        entry = {"n": n, "value": 1e3 / ms, "us_per_round_trip": 1e3 * ms, "timed_round_trips": reps * sets,
+                 "clocks": clk, "l2": f"{sets} buffer sets rotate ({sets * byts / 1e6:.0f} MB > 126 MB L2)",
+                 "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak, "bytes_per_round_trip": byts,
+                              "achieved": byts / (ms * 1e-3) / 1e9, "frac": byts / (ms * 1e-3) / 1e9 / peak,
+                              "note": "compulsory bytes of the two transforms; the row-column intermediates "
+                                      "are not counted"}}
+        if n == 1000:
+            spec_ref = O.fwd(O.real_to_padded(x, dims), dims, dims)
+            spec_got = specs[0].cpu().numpy()[: 2 * w * n].view(np.complex64).reshape(spec_ref.shape)
+            back_got = O.real_from_padded(outs[0].cpu().numpy(), dims)[0]
+            entry["accuracy"] = {"spectrum_rel_l2_vs_fp64": O.rel_l2(spec_got, spec_ref),
+                                 "round_trip_rel_l2_vs_fp64": O.rel_l2(back_got, x * float(n * n))}
+        res[f"n{n}"] = entry
+        del ft, ins, specs, outs
+    res["n1000_over_n1024_time"] = res["n1000"]["us_per_round_trip"] / res["n1024"]["us_per_round_trip"]
+    return res
+
+
 def run_3d(dev, local, min_seconds):
     """64^3 N(0,1) zero-padded to a 256^3 R2C (FwdFFT), then the 256^3 C2R keeping the
     central 128^3 (InvFFT with the output origin at 64^3), batch 1.  Three buffer sets
@@ -993,6 +1058,7 @@ def run_ours(args, world, rank, local):
     # ---- the other workload families (rank 0) ----
     round_trip_2d = run_round_trip_2d(dev, local, args.leg_seconds) if extra else None
     volume_3d = run_3d(dev, local, args.leg_seconds) if extra else None
+    any_length_2d = run_any_length_2d(dev, local, args.leg_seconds) if extra else None
 
     # ---- uneven batch (rank 0): FP32 and BF16 storage ----
     uneven = None
@@ -1106,7 +1172,7 @@ def run_ours(args, world, rank, local):
             "clocks": clk,
             "cufft": cufft,
             "accuracy": accuracy,
-            "round_trip_2d": round_trip_2d, "volume_3d": volume_3d,
+            "round_trip_2d": round_trip_2d, "volume_3d": volume_3d, "any_length_2d": any_length_2d,
             "uneven_batch": uneven, "low_precision_storage": low, "low_precision_tc": low_tc,
             "tensor_core_split": tensor_core, "plain_api": plain,
         }

@@ -352,6 +352,13 @@ fastfft_status allocate(fastfft_plan_s* h) {
     h->dev_err = reinterpret_cast<int*>(static_cast<char*>(h->buffer) + need - 256);
     e = cudaMemset(h->dev_err, 0, sizeof(int));
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemset of the status word");
+    // the chirp-z tables of the plan's lengths, built here rather than at a first launch
+    // that a stream capture may hold
+    const long long lens[4] = {std::max(h->fwd_in.x, h->fwd_out.x), std::max(h->fwd_in.y, h->fwd_out.y), h->inv_in.x,
+                               h->inv_in.y};
+    for (long long n : lens)
+        if (h->rank == 2 && ffb::is_blue_size((int)n) && (e = ffb::prepare_blue_tables((int)n)) != cudaSuccess)
+            return cuda_fail(h, e, "chirp-z tables");
     return FASTFFT_OK;
 }
 

@@ -184,6 +184,12 @@ cudaError_t cols_m(int mode, int dtype, const ColArgs& a, const BlueArgs& b, cud
 
 }  // namespace
 
+cudaError_t prepare_blue_tables(int n) {
+    if (!is_blue_size(n)) return cudaErrorInvalidValue;
+    BlueArgs b;
+    return blue_tables(n, &b);
+}
+
 #define FFB_BLUE_M_SWITCH(n, FN, ...)                  \
     switch (blue_m(n)) {                               \
         case 64: return FN<64>(__VA_ARGS__);           \
