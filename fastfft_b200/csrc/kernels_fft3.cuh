@@ -18,11 +18,16 @@
 namespace ffb {
 
 // Resident threads per SM the register budget of the column passes (batched and single) is
-// sized for: 384 (168 registers), as 4 blocks of one 1536-point FFT (96 threads) each.  Small
-// blocks beat 2 blocks of 2 FFTs (named barriers per FFT) on B200: 5.66 instead of 5.94 us per
-// template at 1536 points in the batched pass, 1.41 instead of 1.58 at 768; a budget of 576
-// threads (96 registers) spills and loses at 1536.
-constexpr int kXcorr3SmThreads = 384;
+// sized for: 480 (at most 136 registers; 128 used at 1536 points without spills), as 5 blocks
+// of one 1536-point FFT (96 threads) each.  Small blocks beat 2 blocks of 2 FFTs (named
+// barriers per FFT) on B200: 5.66 instead of 5.94 us per template at 1536 points in the
+// batched pass, 1.41 instead of 1.58 at 768.  Budgets measured side by side at 1536 points
+// (batched pass, us per template): 384 threads (156 registers, 4 blocks) 5.41-5.53, 480 (128
+// registers, 5 blocks) 5.12, 576 (96 registers, a few spills in other instantiations) 5.15-5.16.
+#ifndef FFB_XCORR3_SM_THREADS
+#define FFB_XCORR3_SM_THREADS 480
+#endif
+constexpr int kXcorr3SmThreads = FFB_XCORR3_SM_THREADS;
 
 // ---------------------------------------------------------------------------
 // Row R2C (forward)
