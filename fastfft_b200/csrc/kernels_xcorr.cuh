@@ -63,9 +63,14 @@ struct XcorrSmem {
 // Block size of the batched column pass: 128 threads (several FFTs per block below N = 2048),
 // with registers budgeted for 512 resident threads per SM.  Smaller blocks than the former 256
 // threads measured faster on B200: 2.06 instead of 2.18 us per template at 1024^2, 0.23
-// instead of 0.32 at 256^2 (64 per launch).
+// instead of 0.32 at 256^2 (64 per launch).  Budgets of 640 (92 registers at 1024) and 768
+// (80) measured on the uneven batch: 383,887-387,140 and 373,363-373,437 templates/s against
+// 385,195-385,889 with 512.
 constexpr int kXcorrBlockThreads = 128;
-constexpr int kXcorrSmThreads = 512;
+#ifndef FFB_XCORR_SM_THREADS
+#define FFB_XCORR_SM_THREADS 512
+#endif
+constexpr int kXcorrSmThreads = FFB_XCORR_SM_THREADS;
 
 // MUL: apply the conj-multiply intra-op (CONJ_MUL or CONJ_MUL_THEN_SCALE; the scale is
 // 1 for CONJ_MUL, an exact multiplication); without it the kernel is a forward/inverse
