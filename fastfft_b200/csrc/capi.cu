@@ -159,15 +159,18 @@ fastfft_status validate(fastfft_plan_s* h) {
     if (dim != h->rank) return fail(h, FASTFFT_ERR_INVALID_DIMS, "plan dimensionality does not match the handle rank");
     // transform lengths: powers of two (FastFFT.cu:895-927); real-input 2D plans also take
     // 3 * 2^k with 128 <= 2^k <= 2048 (384 ... 6144), 5 * 2^k with 128 <= 2^k <= 1024
-    // (640 ... 5120) and 7 * 2^k with 128 <= 2^k <= 512 (896 ... 3584), and any other length
-    // in [17, 4096] (chirp-z on a power-of-two FFT), which the reference rejects
+    // (640 ... 5120) and 7 * 2^k with 128 <= 2^k <= 512 (896 ... 3584); 2D plans, real or
+    // complex input, any other length in [17, 4096] (chirp-z on a power-of-two FFT); the
+    // reference rejects all of these
     const bool wide = dim == 2 && !cplx_dtype(h->input_dtype);
     auto len_ok = [&](long long v) {
-        return is_pow2(v) || (wide && v <= 6144 && (ffb::is_rp_size((int)v) || ffb::is_blue_size((int)v)));
+        return is_pow2(v) || (wide && v <= 6144 && ffb::is_rp_size((int)v)) ||
+               (dim == 2 && ffb::is_blue_size((int)v));
     };
-    const char* lens = wide ? "powers of 2, 3 * 2^k (384 ... 6144), 5 * 2^k (640 ... 5120), 7 * 2^k (896 ... 3584) "
-                              "or any length in [17, 4096]"
-                            : "powers of 2";
+    const char* lens = wide       ? "powers of 2, 3 * 2^k (384 ... 6144), 5 * 2^k (640 ... 5120), 7 * 2^k (896 ... 3584) "
+                                    "or any length in [17, 4096]"
+                       : dim == 2 ? "powers of 2 or any length in [17, 4096]"
+                                  : "powers of 2";
     if ((!len_ok(fi.x) || !len_ok(fi.y) || !is_pow2(fi.z)) && h->fwd_change != SizeChange::Increase)
         return fail(h, FASTFFT_ERR_INVALID_DIMS,
                     std::string("input dimensions must be ") + lens + " unless the forward transform pads");

@@ -9,6 +9,8 @@
 //   blue_r2c_rows_kernel : row R2C, two real rows per complex DFT, transposed [kx][y] output
 //   blue_c2r_rows_kernel : row C2R from [kx][y], two rows per complex DFT, window [X0, X0 + W)
 //   blue_cols_kernel     : column DFT (2D layout), forward / inverse / correlation, window
+//   blue_c2c_rows_fwd_kernel, blue_c2c_rows_inv_kernel : complex-input rows (C2C plans), one row
+//                          per block, transposed [kx][y] output / gather over every kx
 #pragma once
 
 #include "kernels_2d.cuh"
@@ -204,6 +206,66 @@ blue_cols_kernel(ColArgs a, BlueArgs b) {
             const float2 x = (a.out_scale != 1.f) ? cscale(v[q], a.out_scale) : v[q];
             st_cplx<OutC>(pout + n * es, x);
         }
+    }
+}
+
+// Complex-input row forward: row blockIdx.x of batch entry blockIdx.y, X[k] for k < kmax at
+// out[k * out_pitch + row].
+template <int M, class InC>
+__global__ void __launch_bounds__(M / 16)
+blue_c2c_rows_fwd_kernel(RowFwdArgs a, BlueArgs b) {
+    constexpr int T = M / 16;
+    extern __shared__ float2 smem[];
+    using G = FftGroup<M, 1, true>;
+    const int j = threadIdx.x;
+    G g(smem, 0);
+    const int gb = blockIdx.y;
+    const int row = blockIdx.x;
+    const int N = b.n;
+    const int L = min(a.L, N);
+    const InC* p = static_cast<const InC*>(a.in[gb]) + input_row(row, a.rows_y, a.rows_z) * a.in_pitch;
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int n = j + T * q;
+        const float2 x = n < L ? ld_cplx<InC>(p + n) : make_float2(0.f, 0.f);
+        v[q] = (a.scale != 1.f) ? cscale(x, a.scale) : x;
+    }
+    bluestein_dft<M>(v, g, j, a.tw, b, false, leading_slots<T>(L, j), min(N, a.kmax));
+    float2* const o = a.out + (long long)gb * a.out_batch_stride + row;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int k = j + T * q;
+        if (k < a.kmax && k < N) o[(long long)k * a.out_pitch] = v[q];
+    }
+}
+
+// Complex-output row inverse: row blockIdx.x gathers X[k], k < N, from in[k * in_pitch + row]
+// and keeps the outputs [X0, X0 + W).
+template <int M, class OutC>
+__global__ void __launch_bounds__(M / 16)
+blue_c2c_rows_inv_kernel(RowInvArgs a, BlueArgs b) {
+    constexpr int T = M / 16;
+    extern __shared__ float2 smem[];
+    using G = FftGroup<M, 1, true>;
+    const int j = threadIdx.x;
+    G g(smem, 0);
+    const int gb = blockIdx.y;
+    const int row = blockIdx.x;
+    const int N = b.n;
+    const float2* p = a.in + (long long)gb * a.in_batch_stride + row;
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int k = j + T * q;
+        v[q] = k < N ? p[(long long)k * a.in_pitch] : make_float2(0.f, 0.f);
+    }
+    bluestein_dft<M>(v, g, j, a.tw, b, true, 16, min(N, a.X0 + a.W));
+    OutC* o = static_cast<OutC*>(a.out[gb]) + (long long)row * a.out_pitch;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const int n = j + T * q - a.X0;
+        if (n >= 0 && n < a.W && j + T * q < N) st_cplx<OutC>(o + n, (a.scale != 1.f) ? cscale(v[q], a.scale) : v[q]);
     }
 }
 

@@ -49,6 +49,8 @@ cudaError_t launch_xcorr1536_tc(int img_dtype, const XcorrColArgs& a, cudaStream
 cudaError_t launch_blue_r2c(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
 cudaError_t launch_blue_c2r(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
 cudaError_t launch_blue_cols(int n, int mode, int dtype, const ColArgs& a, cudaStream_t st);
+cudaError_t launch_blue_c2c_fwd(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
+cudaError_t launch_blue_c2c_inv(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);
 // Builds (once per device and length, synchronously) the chirp and filter tables of length n.
 cudaError_t prepare_blue_tables(int n);
 

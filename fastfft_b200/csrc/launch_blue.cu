@@ -125,6 +125,28 @@ cudaError_t c2r_impl(const RowInvArgs& a, const BlueArgs& b, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <int M, class InC>
+cudaError_t c2c_fwd_impl(const RowFwdArgs& a, const BlueArgs& b, cudaStream_t st) {
+    static std::atomic<int> hw[64];
+    auto fn = blue_c2c_rows_fwd_kernel<M, InC>;
+    cudaError_t e = ensure_smem_at_least((const void*)fn, blue_smem<M>(), hw);
+    if (e != cudaSuccess) return e;
+    if (a.n_rows == 0) return cudaSuccess;
+    fn<<<dim3(a.n_rows, a.n_batch), M / 16, blue_smem<M>(), st>>>(a, b);
+    return cudaGetLastError();
+}
+
+template <int M, class OutC>
+cudaError_t c2c_inv_impl(const RowInvArgs& a, const BlueArgs& b, cudaStream_t st) {
+    static std::atomic<int> hw[64];
+    auto fn = blue_c2c_rows_inv_kernel<M, OutC>;
+    cudaError_t e = ensure_smem_at_least((const void*)fn, blue_smem<M>(), hw);
+    if (e != cudaSuccess) return e;
+    if (a.n_rows == 0) return cudaSuccess;
+    fn<<<dim3(a.n_rows, a.n_batch), M / 16, blue_smem<M>(), st>>>(a, b);
+    return cudaGetLastError();
+}
+
 template <int M, int MODE, class InC, class ImgC, class OutC>
 cudaError_t cols_impl(const ColArgs& a, const BlueArgs& b, cudaStream_t st) {
     static std::atomic<int> hw[64];
@@ -151,6 +173,25 @@ cudaError_t c2r_m(int out_dtype, const RowInvArgs& a, const BlueArgs& b, cudaStr
         case 0: return c2r_impl<M, float>(a, b, st);
         case 1: return c2r_impl<M, __half>(a, b, st);
         case 2: return c2r_impl<M, __nv_bfloat16>(a, b, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+// complex storage: 3 float2, 4 __half2, 5 __nv_bfloat162
+template <int M>
+cudaError_t c2c_fwd_m(int in_dtype, const RowFwdArgs& a, const BlueArgs& b, cudaStream_t st) {
+    switch (in_dtype) {
+        case 3: return c2c_fwd_impl<M, float2>(a, b, st);
+        case 4: return c2c_fwd_impl<M, __half2>(a, b, st);
+        case 5: return c2c_fwd_impl<M, __nv_bfloat162>(a, b, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <int M>
+cudaError_t c2c_inv_m(int out_dtype, const RowInvArgs& a, const BlueArgs& b, cudaStream_t st) {
+    switch (out_dtype) {
+        case 3: return c2c_inv_impl<M, float2>(a, b, st);
+        case 4: return c2c_inv_impl<M, __half2>(a, b, st);
+        case 5: return c2c_inv_impl<M, __nv_bfloat162>(a, b, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -218,6 +259,22 @@ cudaError_t launch_blue_c2r(int n, int out_dtype, const RowInvArgs& a, cudaStrea
     cudaError_t e = blue_tables(n, &b);
     if (e != cudaSuccess) return e;
     FFB_BLUE_M_SWITCH(n, c2r_m, out_dtype, a, b, st)
+}
+
+cudaError_t launch_blue_c2c_fwd(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st) {
+    if (!is_blue_size(n) || a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
+    BlueArgs b;
+    cudaError_t e = blue_tables(n, &b);
+    if (e != cudaSuccess) return e;
+    FFB_BLUE_M_SWITCH(n, c2c_fwd_m, in_dtype, a, b, st)
+}
+
+cudaError_t launch_blue_c2c_inv(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st) {
+    if (!is_blue_size(n) || a.peaks || a.mip || a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
+    BlueArgs b;
+    cudaError_t e = blue_tables(n, &b);
+    if (e != cudaSuccess) return e;
+    FFB_BLUE_M_SWITCH(n, c2c_inv_m, out_dtype, a, b, st)
 }
 
 cudaError_t launch_blue_cols(int n, int mode, int dtype, const ColArgs& a, cudaStream_t st) {

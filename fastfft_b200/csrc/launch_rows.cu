@@ -96,6 +96,7 @@ static cudaError_t c2c_fwd_dispatch(int in_dtype, const RowFwdArgs& a, cudaStrea
 }
 
 cudaError_t launch_c2c_rows_fwd(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st) {
+    if (is_blue_size(n)) return launch_blue_c2c_fwd(n, in_dtype, a, st);
     FFB_SIZE_SWITCH(n, c2c_fwd_dispatch, in_dtype, a, st)
 }
 
@@ -126,6 +127,7 @@ static cudaError_t c2c_inv_dispatch(int out_dtype, const RowInvArgs& a, cudaStre
 }
 
 cudaError_t launch_c2c_rows_inv(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st) {
+    if (is_blue_size(n)) return launch_blue_c2c_inv(n, out_dtype, a, st);
     FFB_SIZE_SWITCH(n, c2c_inv_dispatch, out_dtype, a, st)
 }
 

@@ -202,3 +202,18 @@ def test_complex_input_rules():
     with pytest.raises(ValueError):
         real.SetOutputDtype("complex64")
     assert C.lib().fastfft_set_output_dtype(real._h, C.DTYPE_C64) == C.ERR_INVALID_ARGUMENT
+
+
+def test_complex_input_lengths_in_2d():
+    """Complex-input 2D plans take any length in [17, 4096] (chirp-z) besides powers of two;
+    3 * 2^k and 3D plans at other lengths stay rejected."""
+    ft = new(input_dtype="complex64")
+    ft.SetForwardFFTPlan(77, 53, 1, 999, 1001, 1)
+    ft.SetInverseFFTPlan(999, 1001, 1, 700, 600, 1)
+    assert ft.ReturnFwdOutputDimensions()[:3] == (999, 1001, 1)
+    for fout, rank in (((384, 384, 1), 2), ((100, 100, 100), 3)):
+        ft = new(rank=rank, input_dtype="complex64")
+        ft.SetForwardFFTPlan(16, 16, fout[2] if rank == 3 else 1, *fout)
+        with pytest.raises(F.FastFFTError) as e:
+            ft.SetInverseFFTPlan(*fout, *fout)
+        assert e.value.status == C.ERR_INVALID_DIMS

@@ -5,7 +5,8 @@ with power-of-two axes, the shortest and longest lengths, forward decrease), inv
 window origin, round trip, the fused correlation through single and batched calls (the
 batched call runs at the plan's size when an axis would correlate at a chirp-z length, and
 through the reduced-size path when both axes correlate at a power of two or 3 * 2^k), the
-half-precision storage types, and the refusal of the fused peak search at such lengths.
+half-precision storage types, the refusal of the fused peak search at such lengths, and
+complex-input (C2C) plans: forward, inverse with an origin, correlation.
 """
 import numpy as np
 import pytest
@@ -188,3 +189,73 @@ def test_peak_search_refused_at_chirp_z_inverse_rows(torch_cuda):
     with pytest.raises(F.FastFFTError) as e:
         ft.FwdImageInvFFTManyPeaks(ins, d_spec, peaks)
     assert e.value.status == C.ERR_UNSUPPORTED
+
+
+# ---- complex input (C2C plans) at chirp-z lengths ----
+def _crand(shape, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def _cmake(fin, fout, iout, origin=None):
+    ft = F.FourierTransformer(input_dtype="complex64")
+    ft.SetForwardFFTPlan(*fin, *fout)
+    ft.SetInverseFFTPlan(*fout, *iout)
+    if origin is not None:
+        ft.SetInverseOutputOrigin(*origin)
+    return ft
+
+
+def _cbuf(torch, a, n_elems=None):
+    return dev(torch, O.complex_to_buffer(a).view(np.float32), n_elems)
+
+
+@pytest.mark.parametrize("fin,fout", [
+    ((77, 53, 1), (999, 1001, 1)),
+    ((1000, 1000, 1), (1000, 1000, 1)),
+    ((100, 30, 1), (300, 512, 1)),           # chirp-z rows, power-of-two columns
+    ((1000, 600, 1), (300, 200, 1)),         # forward decrease
+])
+def test_forward_c2c(torch_cuda, fin, fout):
+    torch = torch_cuda
+    x = _crand((1, fin[1], fin[0]), fin[0] + fout[1])
+    ft = _cmake(fin, fout, fout)
+    out = empty(torch, ft.ReturnFwdOutputMemorySize(), torch.float32)
+    ft.FwdFFT(_cbuf(torch, x), out, pre_op=F.KernelFunction.scale(0.5))
+    ref = O.fwd_c2c(x, fin, fout, pre_op=(O.OP_SCALE, 0.5))
+    got = host(out)[: 2 * ref.size].view(np.complex64).reshape(ref.shape)
+    assert O.rel_l2(got, ref) <= RTOL_L2_BLUE
+    assert O.rel_max(got, ref) <= RTOL_MAX_BLUE
+
+
+@pytest.mark.parametrize("iin,iout,org", [
+    ((999, 1001, 1), (700, 800, 1), (10, 20, 0)),
+    ((1000, 512, 1), (1000, 512, 1), (0, 0, 0)),
+])
+def test_inverse_c2c(torch_cuda, iin, iout, org):
+    torch = torch_cuda
+    spec = _crand((1, iin[0], iin[1]), iin[0] + 3)     # [kz][kx][ky]
+    ft = _cmake(iin, iin, iout, origin=org)
+    out = empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32)
+    ft.InvFFT(_cbuf(torch, spec), out, post_op=F.KernelFunction.scale(0.25))
+    ref = O.inv_c2c(spec, iin, iout, post_op=(O.OP_SCALE, 0.25), origin=org)
+    got = O.complex_from_buffer(host(out), iout)
+    assert O.rel_l2(got, ref) <= RTOL_L2_BLUE
+    assert O.rel_max(got, ref) <= RTOL_MAX_BLUE
+
+
+def test_correlation_c2c(torch_cuda):
+    torch = torch_cuda
+    fin, fout, iout = (100, 80, 1), (1000, 1000, 1), (700, 600, 1)
+    t = _crand((1, fin[1], fin[0]), 21)
+    img = _crand((1, fout[1], fout[0]), 22)
+    spec = O.fwd_c2c(img, fout, fout).astype(np.complex64)
+    ft = _cmake(fin, fout, iout)
+    out = empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32)
+    ft.FwdImageInvFFT(_cbuf(torch, t), dev(torch, spec.view(np.float32)), out)
+    p = O.Plan(fin, fout, fout, iout)
+    ref = O.fwd_image_inv_c2c(t, spec, p)
+    got = O.complex_from_buffer(host(out), iout)
+    assert O.rel_l2(got, ref) <= RTOL_L2_BLUE
+    assert O.rel_max(got, ref) <= RTOL_MAX_BLUE
+    assert int(np.argmax(np.abs(got).ravel())) == int(np.argmax(np.abs(ref).ravel()))
