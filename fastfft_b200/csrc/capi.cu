@@ -159,24 +159,22 @@ fastfft_status validate(fastfft_plan_s* h) {
     if (dim != h->rank) return fail(h, FASTFFT_ERR_INVALID_DIMS, "plan dimensionality does not match the handle rank");
     // transform lengths: powers of two (FastFFT.cu:895-927); real-input 2D plans also take
     // 3 * 2^k with 128 <= 2^k <= 2048 (384 ... 6144), 5 * 2^k with 128 <= 2^k <= 1024
-    // (640 ... 5120) and 7 * 2^k with 128 <= 2^k <= 512 (896 ... 3584); 2D plans, real or
-    // complex input, any other length in [17, 4096] (chirp-z on a power-of-two FFT); the
-    // reference rejects all of these
+    // (640 ... 5120) and 7 * 2^k with 128 <= 2^k <= 512 (896 ... 3584); every plan, real or
+    // complex input, 2D or 3D, any other length in [17, 4096] (chirp-z on a power-of-two FFT;
+    // 3D plans stay within 512 per axis); the reference rejects all of these
     const bool wide = dim == 2 && !cplx_dtype(h->input_dtype);
     auto len_ok = [&](long long v) {
-        return is_pow2(v) || (wide && v <= 6144 && ffb::is_rp_size((int)v)) ||
-               (dim == 2 && ffb::is_blue_size((int)v));
+        return is_pow2(v) || (wide && v <= 6144 && ffb::is_rp_size((int)v)) || ffb::is_blue_size((int)v);
     };
-    const char* lens = wide       ? "powers of 2, 3 * 2^k (384 ... 6144), 5 * 2^k (640 ... 5120), 7 * 2^k (896 ... 3584) "
-                                    "or any length in [17, 4096]"
-                       : dim == 2 ? "powers of 2 or any length in [17, 4096]"
-                                  : "powers of 2";
-    if ((!len_ok(fi.x) || !len_ok(fi.y) || !is_pow2(fi.z)) && h->fwd_change != SizeChange::Increase)
+    const char* lens = wide ? "powers of 2, 3 * 2^k (384 ... 6144), 5 * 2^k (640 ... 5120), 7 * 2^k (896 ... 3584) "
+                              "or any other length in [17, 4096]"
+                            : "powers of 2 or any other length in [17, 4096] (no 3 * 2^k, 5 * 2^k, 7 * 2^k)";
+    if ((!len_ok(fi.x) || !len_ok(fi.y) || !len_ok(fi.z)) && h->fwd_change != SizeChange::Increase)
         return fail(h, FASTFFT_ERR_INVALID_DIMS,
                     std::string("input dimensions must be ") + lens + " unless the forward transform pads");
-    if (!len_ok(fo.x) || !len_ok(fo.y) || !is_pow2(fo.z))
+    if (!len_ok(fo.x) || !len_ok(fo.y) || !len_ok(fo.z))
         return fail(h, FASTFFT_ERR_INVALID_DIMS, std::string("forward output dimensions must be ") + lens);
-    if ((!len_ok(io.x) || !len_ok(io.y) || !is_pow2(io.z)) && h->inv_change != SizeChange::Decrease)
+    if ((!len_ok(io.x) || !len_ok(io.y) || !len_ok(io.z)) && h->inv_change != SizeChange::Decrease)
         return fail(h, FASTFFT_ERR_INVALID_DIMS,
                     std::string("output dimensions must be ") + lens + " unless the inverse transform crops");
     // transform sizes handled by the block FFTs
@@ -357,10 +355,10 @@ fastfft_status allocate(fastfft_plan_s* h) {
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemset of the status word");
     // the chirp-z tables of the plan's lengths, built here rather than at a first launch
     // that a stream capture may hold
-    const long long lens[4] = {std::max(h->fwd_in.x, h->fwd_out.x), std::max(h->fwd_in.y, h->fwd_out.y), h->inv_in.x,
-                               h->inv_in.y};
+    const long long lens[6] = {std::max(h->fwd_in.x, h->fwd_out.x), std::max(h->fwd_in.y, h->fwd_out.y),
+                               std::max(h->fwd_in.z, h->fwd_out.z), h->inv_in.x, h->inv_in.y, h->inv_in.z};
     for (long long n : lens)
-        if (h->rank == 2 && ffb::is_blue_size((int)n) && (e = ffb::prepare_blue_tables((int)n)) != cudaSuccess)
+        if (ffb::is_blue_size((int)n) && (e = ffb::prepare_blue_tables((int)n)) != cudaSuccess)
             return cuda_fail(h, e, "chirp-z tables");
     return FASTFFT_OK;
 }

@@ -8,7 +8,8 @@
 // the same argument structures and layouts as the power-of-two passes in kernels_2d.cuh):
 //   blue_r2c_rows_kernel : row R2C, two real rows per complex DFT, transposed [kx][y] output
 //   blue_c2r_rows_kernel : row C2R from [kx][y], two rows per complex DFT, window [X0, X0 + W)
-//   blue_cols_kernel     : column DFT (2D layout), forward / inverse / correlation, window
+//   blue_cols_kernel     : column DFT, forward / inverse / correlation, window (the general
+//                          column addressing of ColArgs: 2D and 3D passes)
 //   blue_c2c_rows_fwd_kernel, blue_c2c_rows_inv_kernel : complex-input rows (C2C plans), one row
 //                          per block, transposed [kx][y] output / gather over every kx
 #pragma once
@@ -156,7 +157,7 @@ blue_c2r_rows_kernel(RowInvArgs a, BlueArgs b) {
     }
 }
 
-// MODE: COL_FWD, COL_INV or COL_XCORR (forward, conj(T) x image, inverse); 2D layout only.
+// MODE: COL_FWD, COL_INV or COL_XCORR (forward, conj(T) x image, inverse).
 template <int M, int MODE, class InC, class ImgC, class OutC>
 __global__ void __launch_bounds__(M / 16)
 blue_cols_kernel(ColArgs a, BlueArgs b) {
@@ -169,7 +170,9 @@ blue_cols_kernel(ColArgs a, BlueArgs b) {
     const long long bz = blockIdx.y;
     const int N = b.n;
     const int L = min(a.L, N);
-    const InC* pin = static_cast<const InC*>(a.in) + bz * a.in_batch_stride + (long long)col * a.in_stride;
+    const int in_div = a.in_div > 0 ? a.in_div : 1;
+    const InC* pin = static_cast<const InC*>(a.in) + bz * a.in_batch_stride + (long long)(col / in_div) * a.in_stride +
+                     (long long)(col % in_div) * a.in_stride2;
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
@@ -197,7 +200,9 @@ blue_cols_kernel(ColArgs a, BlueArgs b) {
         }
         bluestein_dft<M>(v, g, j, a.tw, b, true, 16, keep);
     }
-    OutC* pout = static_cast<OutC*>(a.out) + bz * a.out_batch_stride + (long long)col * a.out_stride;
+    const int out_div = a.out_div > 0 ? a.out_div : 1;
+    OutC* pout = static_cast<OutC*>(a.out) + bz * a.out_batch_stride + (long long)(col / out_div) * a.out_stride +
+                 (long long)(col % out_div) * a.out_stride2;
     const long long es = a.out_elem_stride > 0 ? a.out_elem_stride : 1;
 #pragma unroll
     for (int q = 0; q < 16; q++) {

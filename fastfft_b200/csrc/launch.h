@@ -44,7 +44,7 @@ bool xcorr1536_tc_supported(const XcorrColArgs& a);
 cudaError_t launch_xcorr1536_tc(int img_dtype, const XcorrColArgs& a, cudaStream_t st);
 
 // Any other length in [17, 4096] (kernels_blue.cuh, chirp-z on a power-of-two FFT): row R2C,
-// row C2R (no peak search or projection), column passes of the 2D layout.  The caller's `tw`
+// row C2R (no peak search or projection), complex rows, column passes (2D and 3D addressing).  The caller's `tw`
 // is the table twiddles_for(n) returns (of the power-of-two length the path runs on).
 cudaError_t launch_blue_r2c(int n, int in_dtype, const RowFwdArgs& a, cudaStream_t st);
 cudaError_t launch_blue_c2r(int n, int out_dtype, const RowInvArgs& a, cudaStream_t st);

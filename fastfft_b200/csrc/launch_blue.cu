@@ -278,9 +278,7 @@ cudaError_t launch_blue_c2c_inv(int n, int out_dtype, const RowInvArgs& a, cudaS
 }
 
 cudaError_t launch_blue_cols(int n, int mode, int dtype, const ColArgs& a, cudaStream_t st) {
-    // 2D layout only (the 3D passes stay at powers of two)
-    if (!is_blue_size(n) || a.in_div > 1 || a.out_div > 1 || a.n_batch < 1 || a.n_batch > kMaxBatch)
-        return cudaErrorInvalidValue;
+    if (!is_blue_size(n) || a.n_batch < 1 || a.n_batch > kMaxBatch) return cudaErrorInvalidValue;
     BlueArgs b;
     cudaError_t e = blue_tables(n, &b);
     if (e != cudaSuccess) return e;

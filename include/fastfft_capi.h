@@ -87,9 +87,9 @@ FASTFFT_API fastfft_status fastfft_set_forward_plan(fastfft_handle h, size_t ix,
  * (AllocateBufferMemory, FastFFT.cu:210-227).  Transform lengths as ValidateDimensions
  * (FastFFT.cu:803-930): powers of two in [16, 8192]; real-input 2D plans also accept
  * 3 * 2^k (384 ... 6144), 5 * 2^k (640 ... 5120) and 7 * 2^k (896 ... 3584) per axis, and
- * 2D plans (real or complex input) any other length in [17, 4096] (extensions; the last run
- * as chirp-z transforms on a power-of-two FFT of length >= 2N - 1, without the fused peak
- * search or projection). */
+ * every plan (real or complex input, 2D or 3D within 512 per axis) any other length in
+ * [17, 4096] (extensions; the last run as chirp-z transforms on a power-of-two FFT of length
+ * >= 2N - 1, without the fused peak search or projection). */
 FASTFFT_API fastfft_status fastfft_set_inverse_plan(fastfft_handle h, size_t ix, size_t iy, size_t iz, size_t ox, size_t oy,
                                         size_t oz, int is_padded);
 

@@ -64,14 +64,12 @@ def test_memory_sizes_match_reference(fin, fout, iout):
     ((64, 64, 1), (512, 512, 1), (256, 256, 1), (256, 256, 1), C.ERR_INVALID_DIMS),  # fwd out != inv in
     ((64, 128, 1), (128, 64, 1), (128, 64, 1), (128, 64, 1), C.ERR_INVALID_DIMS),    # mixed grow/shrink
     ((64, 64, 1), (10240, 64, 1), (10240, 64, 1), (10240, 64, 1), C.ERR_INVALID_DIMS),  # 5 * 2^k above 5120
-    ((16, 16, 16), (320, 320, 320), (320, 320, 320), (320, 320, 320), C.ERR_INVALID_DIMS),  # 5 * 2^k in 3D
     ((64, 64, 1), (7168, 64, 1), (7168, 64, 1), (7168, 64, 1), C.ERR_INVALID_DIMS),  # 7 * 2^k above 3584
-    ((16, 16, 16), (448, 448, 448), (448, 448, 448), (448, 448, 448), C.ERR_INVALID_DIMS),  # 7 * 2^k in 3D
     ((16, 16, 16), (384, 384, 384), (384, 384, 384), (384, 384, 384), C.ERR_INVALID_DIMS),  # 3 * 2^k in 3D
     ((64, 64, 1), (5000, 64, 1), (5000, 64, 1), (5000, 64, 1), C.ERR_INVALID_DIMS),  # other length above 4096
     ((64, 64, 1), (4097, 4097, 1), (4097, 4097, 1), (4097, 4097, 1), C.ERR_INVALID_DIMS),
     ((8, 8, 1), (12, 12, 1), (12, 12, 1), (12, 12, 1), C.ERR_INVALID_DIMS),  # other length below 17
-    ((16, 16, 16), (100, 100, 100), (100, 100, 100), (100, 100, 100), C.ERR_INVALID_DIMS),  # other length in 3D
+    ((16, 16, 16), (600, 600, 600), (600, 600, 600), (600, 600, 600), C.ERR_INVALID_DIMS),  # 3D above 512
     ((64, 64, 1), (512, 512, 1), (512, 512, 1), (5000, 5000, 1), C.ERR_INVALID_DIMS),  # inverse grows, bad length
     ((64, 64, 64), (1024, 1024, 1024), (1024, 1024, 1024), (1024, 1024, 1024), C.ERR_INVALID_DIMS),  # 3D > 512
     ((64, 64, 1), (16384, 16384, 1), (16384, 16384, 1), (16384, 16384, 1), C.ERR_UNSUPPORTED),  # > 8192
@@ -204,14 +202,18 @@ def test_complex_input_rules():
     assert C.lib().fastfft_set_output_dtype(real._h, C.DTYPE_C64) == C.ERR_INVALID_ARGUMENT
 
 
-def test_complex_input_lengths_in_2d():
-    """Complex-input 2D plans take any length in [17, 4096] (chirp-z) besides powers of two;
-    3 * 2^k and 3D plans at other lengths stay rejected."""
-    ft = new(input_dtype="complex64")
-    ft.SetForwardFFTPlan(77, 53, 1, 999, 1001, 1)
-    ft.SetInverseFFTPlan(999, 1001, 1, 700, 600, 1)
-    assert ft.ReturnFwdOutputDimensions()[:3] == (999, 1001, 1)
-    for fout, rank in (((384, 384, 1), 2), ((100, 100, 100), 3)):
+def test_chirp_z_lengths_complex_and_3d():
+    """Complex-input and 3D plans take any length in [17, 4096] (chirp-z; 3D within 512)
+    besides powers of two; 3 * 2^k stays rejected there."""
+    for fin, fout, iout, rank, dt in (((77, 53, 1), (999, 1001, 1), (700, 600, 1), 2, "complex64"),
+                                      ((16, 16, 16), (100, 60, 50), (100, 60, 50), 3, "float32"),
+                                      ((16, 16, 16), (100, 60, 50), (30, 20, 10), 3, "complex64"),
+                                      ((16, 16, 16), (320, 448, 64), (320, 448, 64), 3, "float32")):
+        ft = new(rank=rank, input_dtype=dt)
+        ft.SetForwardFFTPlan(*fin, *fout)
+        ft.SetInverseFFTPlan(*fout, *iout)
+        assert ft.ReturnFwdOutputDimensions()[:3] == fout
+    for fout, rank in (((384, 384, 1), 2), ((384, 384, 384), 3)):
         ft = new(rank=rank, input_dtype="complex64")
         ft.SetForwardFFTPlan(16, 16, fout[2] if rank == 3 else 1, *fout)
         with pytest.raises(F.FastFFTError) as e:

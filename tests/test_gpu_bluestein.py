@@ -6,7 +6,8 @@ window origin, round trip, the fused correlation through single and batched call
 batched call runs at the plan's size when an axis would correlate at a chirp-z length, and
 through the reduced-size path when both axes correlate at a power of two or 3 * 2^k), the
 half-precision storage types, the refusal of the fused peak search at such lengths, and
-complex-input (C2C) plans: forward, inverse with an origin, correlation.
+complex-input (C2C) plans (forward, inverse with an origin, correlation) and 3D plans
+(forward with padding and decrease, inverse with a central window, correlation, C2C).
 """
 import numpy as np
 import pytest
@@ -259,3 +260,86 @@ def test_correlation_c2c(torch_cuda):
     assert O.rel_l2(got, ref) <= RTOL_L2_BLUE
     assert O.rel_max(got, ref) <= RTOL_MAX_BLUE
     assert int(np.argmax(np.abs(got).ravel())) == int(np.argmax(np.abs(ref).ravel()))
+
+
+# ---- 3D plans at chirp-z lengths (within 512 per axis) ----
+def _make3(fin, fout, iout, origin=None, input_dtype="float32"):
+    ft = F.FourierTransformer(input_dtype=input_dtype, rank=3)
+    ft.SetForwardFFTPlan(*fin, *fout)
+    ft.SetInverseFFTPlan(*fout, *iout)
+    if origin is not None:
+        ft.SetInverseOutputOrigin(*origin)
+    return ft
+
+
+def _spec3(t, dims):
+    x, y, z = dims
+    w, _ = O.padded_x(x)
+    return host(t)[: 2 * w * y * z].view(np.complex64).reshape(z, w, y)
+
+
+@pytest.mark.parametrize("fin,fout", [
+    ((16, 16, 16), (100, 60, 50)),           # chirp-z on every axis
+    ((33, 20, 17), (33, 20, 17)),
+    ((64, 30, 16), (64, 30, 16)),            # power-of-two x and z, chirp-z y
+    ((100, 60, 50), (40, 30, 20)),           # forward decrease
+])
+def test_forward_3d(torch_cuda, fin, fout):
+    torch = torch_cuda
+    x = np.random.default_rng(sum(fin)).standard_normal((fin[2], fin[1], fin[0])).astype(np.float32)
+    ft = _make3(fin, fout, fout)
+    out = empty(torch, ft.ReturnFwdOutputMemorySize(), torch.float32)
+    ft.FwdFFT(dev(torch, O.real_to_padded(x, fin)), out)
+    ref = O.fwd(O.real_to_padded(x, fin), fin, fout)
+    got = _spec3(out, fout)
+    assert O.rel_l2(got, ref) <= RTOL_L2_BLUE
+    assert O.rel_max(got, ref) <= RTOL_MAX_BLUE
+
+
+@pytest.mark.parametrize("iin,iout,org", [
+    ((100, 60, 50), (100, 60, 50), (0, 0, 0)),
+    ((100, 60, 50), (40, 30, 20), (30, 15, 15)),     # central window
+])
+def test_inverse_3d(torch_cuda, iin, iout, org):
+    torch = torch_cuda
+    rng = np.random.default_rng(sum(iin) + sum(iout))
+    w, _ = O.padded_x(iin[0])
+    shape = (iin[2], w, iin[1])
+    spec = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    ft = _make3(iin, iin, iout, origin=org)
+    out = empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32)
+    ft.InvFFT(dev(torch, spec.view(np.float32)), out)
+    got = O.real_from_padded(host(out), iout)
+    ref = O.real_from_padded(O.inv(spec, iin, iout, out_dtype=np.float64, origin=org), iout)
+    assert O.rel_l2(got, ref) <= RTOL_L2_BLUE
+    assert O.rel_max(got, ref) <= RTOL_MAX_BLUE
+
+
+def test_correlation_3d(torch_cuda):
+    torch = torch_cuda
+    fin, fout, iout = (16, 12, 10), (100, 60, 50), (40, 30, 20)
+    rng = np.random.default_rng(8)
+    t = rng.standard_normal((fin[2], fin[1], fin[0])).astype(np.float32)
+    img = rng.standard_normal((fout[2], fout[1], fout[0]))
+    spec = O.fwd(O.real_to_padded(img, fout, dtype=np.float64), fout, fout).astype(np.complex64)
+    ft = _make3(fin, fout, iout)
+    out = empty(torch, ft.ReturnInvOutputMemorySize(), torch.float32)
+    ft.FwdImageInvFFT(dev(torch, O.real_to_padded(t, fin)), dev(torch, spec.view(np.float32)), out)
+    got = O.real_from_padded(host(out), iout)
+    ref = O.real_from_padded(O.fwd_image_inv(O.real_to_padded(t, fin), spec, O.Plan(fin, fout, fout, iout),
+                                             out_dtype=np.float64), iout)
+    assert O.rel_l2(got, ref) <= RTOL_L2_BLUE
+    assert O.rel_max(got, ref) <= RTOL_MAX_BLUE
+
+
+def test_forward_c2c_3d(torch_cuda):
+    torch = torch_cuda
+    fin, fout = (16, 16, 16), (100, 60, 50)
+    x = _crand((fin[2], fin[1], fin[0]), 31)
+    ft = _make3(fin, fout, fout, input_dtype="complex64")
+    out = empty(torch, ft.ReturnFwdOutputMemorySize(), torch.float32)
+    ft.FwdFFT(_cbuf(torch, x), out)
+    ref = O.fwd_c2c(x, fin, fout)
+    got = host(out)[: 2 * ref.size].view(np.complex64).reshape(ref.shape)
+    assert O.rel_l2(got, ref) <= RTOL_L2_BLUE
+    assert O.rel_max(got, ref) <= RTOL_MAX_BLUE
