@@ -111,7 +111,10 @@ r2c3_rows_kernel(RowFwdArgs a) {
 // ---------------------------------------------------------------------------
 // The C2R gathers its input from L2/HBM with all of a thread's loads in flight at once, so it
 // gains from a third resident block per SM (56 registers; measured on B200 at 1536 points:
-// 4.2 instead of 4.6 us per template); the R2C does not, and keeps two.
+// 4.2 instead of 4.6 us per template); the R2C does not, and keeps two.  Measured again with
+// the 1536-point step (us per template): R2C at 3 blocks (56 registers, 48 bytes spilled)
+// 2.086 against 2.093 at 2, within noise; C2R at 4 blocks (40 registers, 104 bytes spilled)
+// 3.96 against 2.81 at 3.
 #ifndef FFB_C2R3_MIN_BLOCKS
 #define FFB_C2R3_MIN_BLOCKS 3
 #endif
