@@ -1185,7 +1185,8 @@ def run_profile_case(case, local, groups=1, per_launch=64):
     1024^2 windows (the bench's step: image preparation, R2C, fused column pass, C2R);
     "single": one FwdImageInvFFT call of that template at the size-4096 kernels;
     "uneven": the 1024-template uneven batch's first 64 templates (FP32); "headline_tc": the
-    headline case with the tensor-core column pass (SetTensorCoreDFT).  groups / per_launch:
+    headline case with the tensor-core column pass (SetTensorCoreDFT); "any_length": two
+    1000^2 R2C + C2R round trips on the chirp-z kernels (no image).  groups / per_launch:
     the headline case's schedule (groups in flight, templates per launch)."""
     import torch
 
@@ -1194,6 +1195,20 @@ def run_profile_case(case, local, groups=1, per_launch=64):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if case == "any_length":
+        n = 1000
+        ft = F.FourierTransformer()
+        ft.SetForwardFFTPlan(n, n, 1, n, n, 1)
+        ft.SetInverseFFTPlan(n, n, 1, n, n, 1)
+        xin = torch.randn(ft.ReturnInputMemorySize(), device=dev)
+        spec = torch.empty(ft.ReturnFwdOutputMemorySize(), device=dev)
+        out = torch.empty(ft.ReturnInvOutputMemorySize(), device=dev)
+        for _ in range(2):
+            ft.FwdFFT(xin, spec)
+            ft.InvFFT(spec, out)
+        torch.cuda.synchronize()
+        print(f"profile case done: {case}", flush=True)
+        return
     prep = F.FourierTransformer()
     prep.SetForwardFFTPlan(N, N, 1, N, N, 1)
     prep.SetInverseFFTPlan(N, N, 1, N, N, 1)
@@ -1252,7 +1267,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-cufft", action="store_true")
     ap.add_argument("--skip-uneven", action="store_true", help="skip the secondary workloads")
-    ap.add_argument("--profile-case", choices=["headline", "headline_tc", "single", "uneven"],
+    ap.add_argument("--profile-case", choices=["headline", "headline_tc", "single", "uneven", "any_length"],
                     help="run one small fixed workload for an ncu capture and exit")
     ap.add_argument("--profile-groups", type=int, default=1, help="groups in flight of the headline profile case")
     ap.add_argument("--profile-per-launch", type=int, default=64, help="templates per launch of that case")
